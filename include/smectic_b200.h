@@ -1,0 +1,136 @@
+/*
+ * smectic_b200.h -- C-ABI of the B200-native smectic3D time loop.
+ *
+ * The reference (evitral/smectic3D) has no library boundary: each program
+ * integrates the Swift-Hohenberg model inside one main().  This header is the
+ * boundary that replaces exactly that loop body and its diagnostics while
+ * keeping main()'s inputs (the compile-time constants, the initial condition)
+ * and outputs (psi in the reference's array layouts, L1, energy, surface
+ * files).  Every entry point returns an int status (SH_OK = 0); no exception or
+ * CUDA type crosses the boundary.  One handle owns its device memory and its
+ * CUDA stream; use one handle per host thread.
+ */
+#ifndef SMECTIC_B200_H
+#define SMECTIC_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SH_OK 0
+#define SH_EINVAL 1        /* bad argument or parameter combination            */
+#define SH_ENOMEM 2        /* device or pinned host allocation failed          */
+#define SH_ENONFINITE 3    /* the state became NaN/Inf                          */
+#define SH_ETIMEOUT 4      /* a bounded device wait gave up                     */
+#define SH_ECUDA 5         /* a CUDA call failed (message in sh_last_error)     */
+#define SH_EUNSUPPORTED 6  /* size / option not built into this library        */
+#define SH_ESTATE 7        /* call out of order (e.g. step before set_psi)      */
+
+/* boundary (transform family) */
+#define SH_PERIODIC 0      /* R2C / C2R  (periodicFFT/pf3d.cpp:226-291)           */
+#define SH_NEUMANN 1       /* REDFT10 / REDFT01 (cosFFT/mesabi/cosNoAdvMorph.cpp:249-262) */
+/* nonlinearity */
+#define SH_QUINTIC 0       /* beta psi^3 - gamma psi^5 (periodicFFT/pf3d.cpp:368-369) */
+#define SH_QUAD_CUBIC 1    /* beta psi^2 - gamma psi^3                           */
+/* time scheme */
+#define SH_CNAB2 0         /* Crank-Nicolson + Adams-Bashforth 2 (periodicFFT/pf3d.cpp:476-478) */
+#define SH_IMEX_EULER 1    /* (psihat + dt Nhat) / (1 - dt L)                     */
+/* arithmetic of fields and transforms */
+#define SH_FP64 0
+#define SH_FP32 1
+/* host array layouts of psi */
+#define SH_LAYOUT_DENSE 0  /* (i*N + j)*N + k       (cosFFT/mesabi/cosNoAdvMorph.cpp:296) */
+#define SH_LAYOUT_PADDED 1 /* (i*N + j)*2(N/2+1) + k (periodicFFT/pf3d.cpp:312)         */
+
+/*
+ * Runtime copy of the constants the reference hard-codes at the top of main()
+ * (periodicFFT/pf3d.cpp:35-73, cosFFT/mesabi/cosNoAdvMorph.cpp:74-112).
+ * dx = L/N = 2 pi / (q0 Nw) in the reference.
+ */
+typedef struct sh_params {
+  int n;             /* grid points per side: 16, 32, 64, 128, 256 or 512   */
+  int batch;         /* independent replicas integrated together (>= 1)     */
+  int boundary;      /* SH_PERIODIC / SH_NEUMANN                             */
+  int advection;     /* 1: Stokes advection (periodic only, pf3d.cpp:399-465) */
+  int nonlinearity;  /* SH_QUINTIC / SH_QUAD_CUBIC                           */
+  int scheme;        /* SH_CNAB2 / SH_IMEX_EULER                             */
+  int precision;     /* SH_FP64 / SH_FP32                                    */
+  int l1_interval;   /* steps between L1 evaluations (pf3d.cpp:489: 100); 0 = off */
+  int energy_trace;  /* 1: record the energy of every new state              */
+  int reserved;
+  double dx, dt, eps, beta, gamma, alpha, q0, eta, rho;
+  double w_mid;      /* pinning penalty weight (periodicFFT/pf3dMorph.cpp:102) */
+  double sub_sigma;  /* substrate penalty sigma (cosFFT/comet/cosNoAdvMorph.cpp:67-74) */
+  double sub_z0;
+  const double* eps_per_replica; /* NULL, or `batch` values of epsilon       */
+} sh_params;
+
+typedef struct sh_handle sh_handle;
+
+/* Fill `p` with the plain periodic 128^3 case (eps=-0.75, beta=2, gamma=1,
+ * alpha=q0=1, dx=2 pi/8, dt=0.05, FP64, CNAB2, quintic). */
+int sh_default_params(sh_params* p);
+
+/* Allocate a solver.  Replaces the set-up part of main(): wavenumbers
+ * (periodicFFT/pf3d.cpp:162-190), operator tables (:195-222, recomputed from
+ * indices on the device) and the FFTW plans (:226-291). */
+int sh_create(const sh_params* p, sh_handle** out);
+int sh_destroy(sh_handle* h);
+
+/* Load psi^0 for all replicas (batch * N^3 values, replica-major) and compute
+ * the first N-hat (Euler start, periodicFFT/pf3d.cpp:363-374). */
+int sh_set_psi(sh_handle* h, const double* host_psi, int layout);
+/* Same, from a device buffer of batch*N^3 doubles (dense layout). */
+int sh_set_psi_device(sh_handle* h, const double* dev_psi);
+/* Copy the current psi out (gathered psi, periodicFFT/pf3d.cpp:554-568). */
+int sh_get_psi(sh_handle* h, double* host_psi, int layout);
+int sh_get_psi_device(sh_handle* h, double* dev_psi);
+
+/* Advance every replica by `nsteps` time steps (the body of the while loop,
+ * periodicFFT/pf3d.cpp:390-550; cosFFT/mesabi/cosNoAdvMorph.cpp:483-620).
+ * Returns after the steps completed; SH_ENONFINITE if psi became NaN/Inf. */
+int sh_step(sh_handle* h, int nsteps);
+/* Enqueue `nsteps` steps on the handle's stream and return immediately. */
+int sh_step_async(sh_handle* h, int nsteps);
+
+/* One drop-in time loop with host buffers: psi0 in, nsteps steps, psi out. */
+int sh_run(sh_handle* h, const double* host_psi0, int nsteps, double* host_psi_out, int layout);
+
+/* Lyapunov energy of the current state, one value per replica
+ * (energyPsi.m:225-234 with the exact spectral Laplacian, FP64 sums). */
+int sh_energy(sh_handle* h, double* out);
+/* Energies recorded by energy_trace: out[s*batch + r] for the first
+ * min(max_steps, steps taken) steps; *count receives the number of steps. */
+int sh_energy_trace(sh_handle* h, double* out, int max_steps, int* count);
+/* Latest L1 monitor values (periodicFFT/pf3d.cpp:489-509), one per replica,
+ * and how many evaluations happened so far. */
+int sh_l1(sh_handle* h, double* out, int* count);
+
+/* surfTrack pass (periodicFFT/surfTrack.cpp:602-626, 767-806): takes one step
+ * and scans every (i, j) column of the new psi for its first crossing.  Writes
+ * N*N values per replica: z index (or -1), v_n, H, K (NaN where no crossing). */
+int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kgauss);
+
+/* Binary checkpoint of the full state (including the AB2 history, which the
+ * reference's text files drop): query size with buf == NULL. */
+int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes);
+int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes);
+
+/* Pinned host memory for fast host<->device copies. */
+int sh_host_alloc(size_t bytes, void** out);
+int sh_host_free(void* p);
+
+int sh_synchronize(sh_handle* h);
+void* sh_stream(sh_handle* h);               /* the handle's cudaStream_t */
+long long sh_steps_taken(sh_handle* h);
+int sh_kernel_launches(sh_handle* h, long long* count);
+const char* sh_last_error(sh_handle* h);     /* NULL handle: last global error */
+const char* sh_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SMECTIC_B200_H */

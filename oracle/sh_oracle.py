@@ -1,0 +1,510 @@
+"""FP64 CPU oracle for the smectic3D per-step Swift-Hohenberg update.
+
+TEST INFRASTRUCTURE ONLY.  This module is the checker that the CUDA path is
+compared against; it is imported by ``tests/``, by ``__graft_entry__.smoke()``
+and by the CPU-baseline leg of ``bench.py`` and by nothing else.  The product
+path never calls it.
+
+It is a line-by-line restatement of the reference's time loops in NumPy/SciPy
+(pocketfft, double precision) in place of FFTW 3.3-MPI, which the reference
+links and which is not available here:
+
+* periodic plain step           periodicFFT/pf3dVal.cpp:247-301
+* periodic advected step        periodicFFT/pf3d.cpp:162-222, 363-485
+* pinning penalty (option)      periodicFFT/pf3dMorph.cpp:456-467, 572-589
+* surfTrack surface pass        periodicFFT/surfTrack.cpp:602-626, 767-806
+* Neumann (DCT) step            cosFFT/mesabi/cosNoAdvMorph.cpp:112, 216-231,
+                                423-442, 483-530
+* substrate penalty (option)    cosFFT/comet/cosNoAdvMorph.cpp:67-74, 480-540,
+                                591-623
+* L1 monitor                    periodicFFT/pf3d.cpp:489-518
+* energy functional             energyPsi.m:217-234 (FD + trapz form) and its
+                                spectral restatement
+
+Parity status: UNPINNED against the reference's own outputs.  The reference
+has no tests, golden files or fixtures and cannot be compiled here (it needs
+fftw3-mpi and an MPI C++ compiler), so no reference output exists to pin
+against.  The oracle is instead pinned to analytic known-answer tests
+(tests/test_oracle.py): transform scale conventions of FFTW's R2C/C2R and
+REDFT10/REDFT01, the exact CNAB2 growth factor of grid modes, the lamellar
+amplitude and Lyapunov decrease, the Stokes projector identities and the
+surfTrack crossing of a planar front.
+
+Conventions kept from the reference:
+* SciPy ``rfftn``/``irfftn`` equal FFTW's unnormalised r2c/c2r, including the
+  c2r treatment of non-Hermitian data on the kz=0 and kz=N/2 planes (complex
+  inverse over x and y, then the real part of those planes).
+* ``dctn(type=2)`` / ``dctn(type=3)`` with norm=None equal REDFT10 / REDFT01.
+* The Nyquist wavenumber is +pi/dx (periodicFFT/pf3d.cpp:166-190).
+* The first step uses N^{-1} := N(psi^0) without advection (Euler start,
+  periodicFFT/pf3d.cpp:363-374).
+"""
+from __future__ import annotations
+
+import dataclasses
+import os
+
+import numpy as np
+import scipy.fft as sfft
+
+WORKERS = os.cpu_count() or 1
+
+
+@dataclasses.dataclass
+class Params:
+    """Runtime copy of the constants the reference hard-codes in main().
+
+    periodicFFT/pf3d.cpp:46-73, cosFFT/mesabi/cosNoAdvMorph.cpp:89-112.
+    """
+    n: int = 32
+    dx: float = 2.0 * np.pi / 8.0
+    dt: float = 0.05
+    eps: float = -0.75
+    beta: float = 2.0
+    gamma: float = 1.0
+    alpha: float = 1.0
+    q0: float = 1.0
+    eta: float = 1.0
+    rho: float = 1.0
+    nonlinearity: str = "quintic"   # "quintic": b psi^3 - g psi^5 ; "quad_cubic": b psi^2 - g psi^3
+    scheme: str = "cnab2"           # "cnab2" (reference) or "imex_euler"
+    w_mid: float = 0.0              # pinning penalty weight (pf3dMorph wMid)
+    sub_sigma: float = 0.0          # substrate penalty sigma (comet cosNoAdvMorph)
+    sub_z0: float = 1e-4
+
+
+# ---------------------------------------------------------------------------
+# wavenumbers
+# ---------------------------------------------------------------------------
+
+def kvec_periodic(n: int, dx: float) -> np.ndarray:
+    """Vq[i] = 2 pi i/(dx N) for i <= N/2, else -(N-i) 2 pi/(dx N).
+
+    periodicFFT/pf3d.cpp:162-190: the Nyquist entry is +pi/dx.
+    """
+    q = np.empty(n)
+    for i in range(n):
+        if i < n // 2 + 1:
+            q[i] = 2.0 * np.pi * i / (dx * n)
+        else:
+            q[i] = -(n - i) * 2.0 * np.pi / (dx * n)
+    return q
+
+
+def kvec_dct(n: int, dx: float) -> np.ndarray:
+    """Vq[m] = pi m/(dx N), cosFFT/mesabi/cosNoAdvMorph.cpp:216-231."""
+    return np.pi * np.arange(n) / (dx * n)
+
+
+def _grids_periodic(p: Params):
+    q = kvec_periodic(p.n, p.dx)
+    qx = q[:, None, None]
+    qy = q[None, :, None]
+    qz = q[None, None, : p.n // 2 + 1]
+    return qx, qy, qz
+
+
+def _grids_dct(p: Params):
+    q = kvec_dct(p.n, p.dx)
+    return q[:, None, None], q[None, :, None], q[None, None, :]
+
+
+def _tables(mq2, p: Params):
+    """opSH, aLin, C1, C2 (periodicFFT/pf3d.cpp:195-216)."""
+    op_sh = p.alpha * (mq2 - p.q0 * p.q0) ** 2
+    a_lin = p.eps - op_sh
+    c1 = 1.0 + 0.5 * p.dt * a_lin
+    c2 = 1.0 - 0.5 * p.dt * a_lin
+    return op_sh, a_lin, c1, c2
+
+
+# ---------------------------------------------------------------------------
+# nonlinearity
+# ---------------------------------------------------------------------------
+
+def nonlin(psi: np.ndarray, p: Params) -> np.ndarray:
+    """N(psi) = beta psi^3 - gamma psi^5 (periodicFFT/pf3d.cpp:368-369).
+
+    ``quad_cubic`` selects beta psi^2 - gamma psi^3 instead.
+    """
+    if p.nonlinearity == "quintic":
+        return p.beta * psi ** 3 - p.gamma * psi ** 5
+    if p.nonlinearity == "quad_cubic":
+        return p.beta * psi ** 2 - p.gamma * psi ** 3
+    raise ValueError(p.nonlinearity)
+
+
+def nonlin_deriv(psi: np.ndarray, p: Params) -> np.ndarray:
+    if p.nonlinearity == "quintic":
+        return 3.0 * p.beta * psi ** 2 - 5.0 * p.gamma * psi ** 4
+    return 2.0 * p.beta * psi - 3.0 * p.gamma * psi ** 2
+
+
+def pin_penalty(psi: np.ndarray, p: Params, dz: float) -> np.ndarray:
+    """2 wMid (psi[k-1] - 2 psi[k] + psi[k+1]) / dz^2 on the plane k = Nz/2.
+
+    periodicFFT/pf3dMorph.cpp:456-467.
+    """
+    out = np.zeros_like(psi)
+    if p.w_mid != 0.0:
+        m = psi.shape[2] // 2
+        out[:, :, m] = 2.0 * p.w_mid * (psi[:, :, m - 1] - 2.0 * psi[:, :, m] + psi[:, :, m + 1]) / (dz * dz)
+    return out
+
+
+# ---------------------------------------------------------------------------
+# periodic solver (R2C / C2R)
+# ---------------------------------------------------------------------------
+
+def r2c(a):
+    return sfft.rfftn(a, workers=WORKERS)
+
+
+def c2r(a, n):
+    """Unnormalised inverse (FFTW c2r convention)."""
+    return sfft.irfftn(a, s=(n, n, n), norm="forward", workers=WORKERS)
+
+
+class PeriodicOracle:
+    """Periodic SH integrator (plain or with Stokes advection).
+
+    State: psi (real, dense (N,N,N)) and NqPast (half spectrum).
+    """
+
+    def __init__(self, psi0: np.ndarray, p: Params, advect: bool = False):
+        self.p = p
+        self.n = p.n
+        self.advect = advect
+        self.scale = 1.0 / float(self.n) ** 3
+        qx, qy, qz = _grids_periodic(p)
+        self.qx, self.qy, self.qz = qx, qy, qz
+        self.mq2 = qx * qx + qy * qy + qz * qz
+        self.op_sh, self.a_lin, self.c1, self.c2 = _tables(self.mq2, p)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            cm1 = 1.0 / (p.rho * p.eta * self.mq2)
+            cm2x = qx / self.mq2
+            cm2y = qy / self.mq2
+            cm2z = qz / self.mq2
+        # periodicFFT/pf3d.cpp:219-222: zero mode of the Stokes tables
+        cm1[0, 0, 0] = 0.0
+        cm2x = np.broadcast_to(cm2x, self.mq2.shape).copy()
+        cm2y = np.broadcast_to(cm2y, self.mq2.shape).copy()
+        cm2z = np.broadcast_to(cm2z, self.mq2.shape).copy()
+        cm2x[0, 0, 0] = cm2y[0, 0, 0] = cm2z[0, 0, 0] = 0.0
+        self.cm1, self.cm2x, self.cm2y, self.cm2z = cm1, cm2x, cm2y, cm2z
+        self.psi = np.array(psi0, dtype=np.float64, copy=True)
+        self.dz = p.dx
+        # First NqPast, discarding advection (periodicFFT/pf3d.cpp:363-374)
+        self.nq_past = r2c(self._nonlin_local(self.psi))
+        self.step_count = 0
+        self.last = {}
+
+    def _nonlin_local(self, psi):
+        return nonlin(psi, self.p) + pin_penalty(psi, self.p, self.dz)
+
+    def velocity(self, psiq):
+        """Stokes velocity from S = (L psi) grad psi.
+
+        periodicFFT/pf3d.cpp:399-451.  Returns (u, grad, lpsi).
+        """
+        n, s = self.n, self.scale
+        gx = c2r(s * 1j * self.qx * psiq, n)
+        gy = c2r(s * 1j * self.qy * psiq, n)
+        gz = c2r(s * 1j * self.qz * psiq, n)
+        lpsi = c2r(s * self.op_sh * psiq, n)
+        sqx = r2c(lpsi * gx)
+        sqy = r2c(lpsi * gy)
+        sqz = r2c(lpsi * gz)
+        dot = self.qx * sqx + self.qy * sqy + self.qz * sqz
+        ux = c2r(s * self.cm1 * (sqx - self.cm2x * dot), n)
+        uy = c2r(s * self.cm1 * (sqy - self.cm2y * dot), n)
+        uz = c2r(s * self.cm1 * (sqz - self.cm2z * dot), n)
+        return (ux, uy, uz), (gx, gy, gz), lpsi
+
+    def step(self):
+        """One time step (periodicFFT/pf3d.cpp:395-485; pf3dVal.cpp:276-301)."""
+        p, n, s = self.p, self.n, self.scale
+        psi = self.psi
+        psiq = r2c(psi)
+        nr = self._nonlin_local(psi)
+        grads = None
+        if self.advect:
+            (ux, uy, uz), grads, _ = self.velocity(psiq)
+            nr = nr - ux * grads[0] - uy * grads[1] - uz * grads[2]
+        nq = r2c(nr)
+        if p.scheme == "cnab2":
+            psiq_new = s * (self.c1 * psiq + 0.5 * p.dt * (3.0 * nq - self.nq_past)) / self.c2
+        elif p.scheme == "imex_euler":
+            psiq_new = s * (psiq + p.dt * nq) / (1.0 - p.dt * self.a_lin)
+        else:
+            raise ValueError(p.scheme)
+        psi_new = c2r(psiq_new, n)
+        self.last = {"psiq": psiq, "nq": nq, "grads": grads, "psi_old": psi}
+        self.nq_past = nq
+        self.psi = psi_new
+        self.step_count += 1
+        return psi_new
+
+    def run(self, steps: int):
+        for _ in range(steps):
+            self.step()
+        return self.psi
+
+    # -- surfTrack --------------------------------------------------------
+    def surface_fields(self):
+        """Spectral fields surfTrack builds in its step.
+
+        periodicFFT/surfTrack.cpp:602-626, using the values of the step just
+        taken (psi^n spectrum, N^n).  The reference builds the curvature
+        spectra from arrays it has already passed to FFTW c2r plans, which
+        FFTW may overwrite; this restates the intended -q_a q_b psiq form.
+        """
+        n, s = self.n, self.scale
+        psiq, nq = self.last["psiq"], self.last["nq"]
+        grads = self.last["grads"]
+        if grads is None:
+            grads = (c2r(s * 1j * self.qx * psiq, n), c2r(s * 1j * self.qy * psiq, n),
+                     c2r(s * 1j * self.qz * psiq, n))
+        dtpsi = c2r(s * (self.a_lin * psiq + nq), n)
+        dxx = c2r(-s * self.qx * self.qx * psiq, n)
+        dyy = c2r(-s * self.qy * self.qy * psiq, n)
+        dxy = c2r(-s * self.qx * self.qy * psiq, n)
+        curvh = c2r(-s * (self.qx * self.qx + self.qy * self.qy) * psiq, n)
+        return grads, dtpsi, curvh, dxx, dyy, dxy
+
+
+def surface_scan(psi_new, grads, dtpsi, curvh, dxx, dyy, dxy, threshold: float = 0.1):
+    """Column scan of surfTrack (periodicFFT/surfTrack.cpp:767-806).
+
+    For each (i, j) scan +z for the first psi < 0 after psi > threshold;
+    step back one voxel if that one is closer to zero.  Returns z (the
+    reference writes the unadjusted k), v_n, H, K per column, NaN / -1 where
+    no crossing exists.
+    """
+    n = psi_new.shape[0]
+    z = -np.ones((n, n), dtype=np.int64)
+    vn = np.full((n, n), np.nan)
+    hh = np.full((n, n), np.nan)
+    kk = np.full((n, n), np.nan)
+    for i in range(n):
+        for j in range(n):
+            col = psi_new[i, j]
+            track = 0
+            for k in range(n):
+                if col[k] > threshold and track == 0:
+                    track = 1
+                if col[k] < 0 and track == 1:
+                    idx = k
+                    if abs(col[k]) > abs(col[k - 1]):
+                        idx = k - 1
+                    z[i, j] = k
+                    gv = np.sqrt(grads[0][i, j, idx] ** 2 + grads[1][i, j, idx] ** 2 + grads[2][i, j, idx] ** 2)
+                    vn[i, j] = dtpsi[i, j, idx] / gv
+                    hh[i, j] = curvh[i, j, idx] / gv
+                    kk[i, j] = (dxx[i, j, idx] * dyy[i, j, idx] - dxy[i, j, idx] ** 2) / (gv * gv)
+                    track = 2
+                    break
+    return z, vn, hh, kk
+
+
+# ---------------------------------------------------------------------------
+# Neumann solver (REDFT10 / REDFT01)
+# ---------------------------------------------------------------------------
+
+def dct3d(a):
+    return sfft.dctn(a, type=2, workers=WORKERS)
+
+
+def idct3d(a):
+    return sfft.dctn(a, type=3, workers=WORKERS)
+
+
+class NeumannOracle:
+    """cosNoAdvMorph: DCT-II forward, DCT-III inverse, scale 0.125/N^3.
+
+    cosFFT/mesabi/cosNoAdvMorph.cpp:112, 216-231, 423-442, 483-530.
+    Substrate penalty: cosFFT/comet/cosNoAdvMorph.cpp:67-74, 591-623.
+    """
+
+    def __init__(self, psi0: np.ndarray, p: Params):
+        self.p = p
+        self.n = p.n
+        self.scale = 0.125 / float(self.n) ** 3
+        qx, qy, qz = _grids_dct(p)
+        self.qx, self.qy, self.qz = qx, qy, qz
+        self.mq2 = qx * qx + qy * qy + qz * qz
+        self.op_sh, self.a_lin, self.c1, self.c2 = _tables(self.mq2, p)
+        self.substrate = -self.scale * (qx * qx + qy * qy)
+        k = np.arange(self.n, dtype=np.float64)
+        # wallPotential(k) = sigma exp(-k/z0) (comet cosNoAdvMorph.cpp:67-74)
+        with np.errstate(over="ignore", under="ignore"):
+            self.wall = (p.sub_sigma * np.exp(-k / p.sub_z0))[None, None, :]
+        self.psi = np.array(psi0, dtype=np.float64, copy=True)
+        self.dz = p.dx
+        self.nq = dct3d(self._nonlin_local(self.psi))
+        self.step_count = 0
+        self.last = {}
+
+    def _nonlin_local(self, psi):
+        out = nonlin(psi, self.p) + pin_penalty(psi, self.p, self.dz)
+        if self.p.sub_sigma != 0.0:
+            pen = idct3d(self.substrate * dct3d(psi))
+            out = out + pen * self.wall
+        return out
+
+    def step(self):
+        p = self.p
+        nq_past = self.nq
+        nq = dct3d(self._nonlin_local(self.psi))
+        psiq = dct3d(self.psi)
+        if p.scheme == "cnab2":
+            psiq_new = self.scale * (self.c1 * psiq + 0.5 * p.dt * (3.0 * nq - nq_past)) / self.c2
+        else:
+            psiq_new = self.scale * (psiq + p.dt * nq) / (1.0 - p.dt * self.a_lin)
+        psi_new = idct3d(psiq_new)
+        self.last = {"psiq": psiq, "nq": nq, "psi_old": self.psi}
+        self.nq = nq
+        self.psi = psi_new
+        self.step_count += 1
+        return psi_new
+
+    def run(self, steps: int):
+        for _ in range(steps):
+            self.step()
+        return self.psi
+
+
+# ---------------------------------------------------------------------------
+# diagnostics
+# ---------------------------------------------------------------------------
+
+def l1_monitor(psi_new, psi_old, dt):
+    """L1 = sum|psiNew - psi| / (dt sum|psiNew|) (periodicFFT/pf3d.cpp:489-509)."""
+    return float(np.abs(psi_new - psi_old).sum() / (dt * np.abs(psi_new).sum()))
+
+
+def _local_density(psi, p: Params):
+    if p.nonlinearity == "quintic":
+        pot = -0.25 * p.beta * psi ** 4 + p.gamma / 6.0 * psi ** 6
+    else:
+        pot = -p.beta / 3.0 * psi ** 3 + 0.25 * p.gamma * psi ** 4
+    return -0.5 * p.eps * psi * psi + pot
+
+
+def energy_spectral_periodic(psi, p: Params) -> float:
+    """Lyapunov functional with the exact (spectral) Laplacian.
+
+    F = dV sum[-eps/2 psi^2 + alpha/2 ((q0^2+lap) psi)^2 - beta/4 psi^4
+    + gamma/6 psi^6], the density of energyPsi.m:225-228 with the periodic
+    sum of the grid in place of trapz and FD.
+    """
+    n = psi.shape[0]
+    dv = p.dx ** 3
+    q = kvec_periodic(n, p.dx)
+    mq2 = q[:, None, None] ** 2 + q[None, :, None] ** 2 + q[None, None, :] ** 2
+    ph = sfft.fftn(psi, workers=WORKERS)
+    grad_term = 0.5 * p.alpha * (np.abs(ph) ** 2 * (p.q0 ** 2 - mq2) ** 2).sum() / n ** 3
+    return float(dv * (_local_density(psi, p).sum() + grad_term))
+
+
+def energy_spectral_neumann(psi, p: Params) -> float:
+    """Same functional with the DCT (Neumann) Laplacian.
+
+    Parseval for REDFT10: sum x^2 = (1/2N) (X0^2/2 + sum_{k>0} Xk^2) per axis.
+    """
+    n = psi.shape[0]
+    dv = p.dx ** 3
+    q = kvec_dct(n, p.dx)
+    mq2 = q[:, None, None] ** 2 + q[None, :, None] ** 2 + q[None, None, :] ** 2
+    x = dct3d(psi)
+    w = np.ones(n)
+    w[0] = 0.5
+    wt = w[:, None, None] * w[None, :, None] * w[None, None, :] / (2.0 * n) ** 3
+    grad_term = 0.5 * p.alpha * (wt * x * x * (p.q0 ** 2 - mq2) ** 2).sum()
+    return float(dv * (_local_density(psi, p).sum() + grad_term))
+
+
+def energy_fd_trapz(psi, p: Params) -> float:
+    """energyPsi.m:131-234 restated: periodic 2nd-order FD Laplacian (:217-219),
+    density (:225-228), triple trapz over xV = 0:dx:L-dx (:234)."""
+    dx2 = 1.0 / p.dx ** 2
+    lap = (np.roll(psi, 1, 0) + np.roll(psi, -1, 0) + np.roll(psi, 1, 1) + np.roll(psi, -1, 1)
+           + np.roll(psi, 1, 2) + np.roll(psi, -1, 2) - 6.0 * psi) * dx2
+    dens = _local_density(psi, p) + 0.5 * p.alpha * (p.q0 ** 2 * psi + lap) ** 2
+    e = np.trapezoid(dens, dx=p.dx, axis=2)
+    e = np.trapezoid(e, dx=p.dx, axis=1)
+    e = np.trapezoid(e, dx=p.dx, axis=0)
+    return float(e)
+
+
+def dominant_wavenumber(psi, dx: float) -> float:
+    """|q| of the shell (width 2 pi/L) holding the most spectral power, DC excluded."""
+    n = psi.shape[0]
+    q = kvec_periodic(n, dx)
+    mq = np.sqrt(q[:, None, None] ** 2 + q[None, :, None] ** 2 + q[None, None, : n // 2 + 1] ** 2)
+    ph = np.abs(r2c(psi)) ** 2
+    w = np.full(n // 2 + 1, 2.0)
+    w[0] = 1.0
+    w[n // 2] = 1.0
+    ph = ph * w[None, None, :]
+    dq = 2.0 * np.pi / (n * dx)
+    shell = np.rint(mq / dq).astype(np.int64)
+    power = np.bincount(shell.ravel(), weights=ph.ravel())
+    power[0] = 0.0
+    return float(np.argmax(power) * dq)
+
+
+# ---------------------------------------------------------------------------
+# discrete adjoint of the plain periodic CNAB2 scheme
+# ---------------------------------------------------------------------------
+
+def adjoint_gradients_periodic(psi0, p: Params, steps: int, target):
+    """Exact discrete adjoint of ``PeriodicOracle`` (plain, CNAB2, no penalty)
+    for L = 1/2 ||psi_T - target||^2 (plain sum over grid points).
+
+    Forward map (real space, A and B symmetric Fourier multipliers):
+        psi^{n+1} = A psi^n + B (3 N(psi^n) - N(psi^{n-1})),  N(psi^{-1}) := N(psi^0)
+        A = F^-1 diag(C1/C2) F,  B = F^-1 diag(dt/2 / C2) F
+    Reverse sweep:
+        lam^T = psi^T - target
+        lam^n = A lam^{n+1} + N'(psi^n) (c_n B lam^{n+1} - B lam^{n+2}),
+        c_n = 3 for n >= 1, c_0 = 2 ; lam^{T+1} = 0.
+    Parameter gradients use d psihat^{n+1}/d a = dt/2 (psihat^n + psihat^{n+1}) / C2
+    with a = aLin, da/d eps = 1, da/d q0 = 4 alpha q0 (|q|^2 - q0^2).
+    Returns (loss, dL/d eps, dL/d q0, dL/d psi0).
+    """
+    assert p.scheme == "cnab2" and p.w_mid == 0.0
+    orc = PeriodicOracle(psi0, p)
+    states = [orc.psi.copy()]
+    for _ in range(steps):
+        states.append(orc.step().copy())
+    n = p.n
+    lam_next = states[-1] - target
+    loss = 0.5 * float((lam_next ** 2).sum())
+    a_mul = orc.c1 / orc.c2
+    b_mul = 0.5 * p.dt / orc.c2
+    da_dq0 = 4.0 * p.alpha * p.q0 * (orc.mq2 - p.q0 ** 2)
+    w = np.full(n // 2 + 1, 2.0)
+    w[0] = 1.0
+    w[n // 2] = 1.0
+    w = w[None, None, :]
+    g_eps = 0.0
+    g_q0 = 0.0
+    blam_next2 = np.zeros((n, n, n))   # B lam^{n+2}
+    for k in range(steps - 1, -1, -1):
+        # lam_next = lam^{k+1}; states[k] = psi^k
+        lq = r2c(lam_next)
+        ph_k = r2c(states[k])
+        ph_k1 = r2c(states[k + 1])
+        dpar = 0.5 * p.dt * (ph_k + ph_k1) / orc.c2
+        # <lam, F^-1 X> = (1/N^3) sum_k w conj(lamhat) X  (real)
+        inner = (w * np.conj(lq) * dpar).real / n ** 3
+        g_eps += float(inner.sum())
+        g_q0 += float((inner * da_dq0).sum())
+        blam = c2r(orc.scale * b_mul * lq, n)
+        alam = c2r(orc.scale * a_mul * lq, n)
+        c = 3.0 if k >= 1 else 2.0
+        lam_k = alam + nonlin_deriv(states[k], p) * (c * blam - blam_next2)
+        blam_next2 = blam
+        lam_next = lam_k
+    return loss, g_eps, g_q0, lam_next

@@ -1,0 +1,315 @@
+// Pencil pass: the x transform, fused with the spectral time update.
+//
+// A CTA owns TK consecutive in-plane positions f (128 bytes of every x-plane
+// row, so each x step is one coalesced segment) and all N values of x.  The
+// forward x transform completes the 3-D spectrum of the nonlinear term; the
+// CNAB2 update runs in registers; the inverse x transform of the new psi
+// spectrum starts from the same registers (the inverse radix plan is the
+// forward plan reversed).
+//
+// The spectral state is W^n = C1 psihat^n - dt/2 Nhat^{n-1}, stored
+// pencil-major ([f][kx], kx contiguous) so that each thread's register slots
+// map to coalesced addresses.  The reference update
+//   psihat^{n+1} = (C1 psihat^n + dt/2 (3 Nhat^n - Nhat^{n-1})) / C2
+// (periodicFFT/pf3d.cpp:476-478, cosFFT/mesabi/cosNoAdvMorph.cpp:524-525)
+// becomes psihat^{n+1} = (W^n + 3 dt/2 Nhat^n) / C2 and
+// W^{n+1} = C1 psihat^{n+1} - dt/2 Nhat^n: one state read and one write.
+#pragma once
+#include "sh_common.cuh"
+
+namespace shb {
+
+enum PencilMode : int { kPencilStep = 0, kPencilInit = 1, kPencilEnergy = 2 };
+
+template <typename T, int N, bool DCT>
+struct PencilCfg {
+  static constexpr int E = Plan<N>::E;
+  static constexpr int G = N / E;
+  static constexpr int TK = sizeof(T) == 4 ? 16 : 8;
+  static constexpr int THREADS = TK * G;
+  static constexpr int LS = line_stride(N);
+  static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
+  static constexpr int TILES = FP / TK;
+  static constexpr int RL = radix_of<N, -1, Plan<N>::P - 1>();
+  static constexpr size_t SMEM = size_t(TK) * LS * sizeof(cplx<T>) + 64 * sizeof(double);
+  static_assert(FP % TK == 0, "tile must divide the plane");
+  static_assert(THREADS % 32 == 0, "pencil CTA must be whole warps");
+};
+
+template <typename T>
+struct PencilArgs {
+  const cplx<T>* src;   // step: partial of N ; init: partial of psi   [rep][x][FP]
+  const cplx<T>* src2;  // init: partial of N(psi)
+  cplx<T>* w;           // state W [rep][FP][N]
+  cplx<T>* dst;         // partial of scale * psihat^{n+1}, x-inverse applied [rep][x][FP]
+  double* red;          // per-CTA spectral energy partial [rep][grid.x]
+  int* nonfinite;       // set to 1 when a new coefficient is NaN/Inf
+  const T* q;           // wavenumber table (N entries)
+  const cplx<T>* tw;
+  const cplx<T>* dtw;
+  PointParams pp;
+  int flags;
+};
+
+template <typename T, int N, bool DCT>
+struct PencilOps {
+  using Cfg = PencilCfg<T, N, DCT>;
+  static constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
+
+  static __device__ __forceinline__ void load_tile(cplx<T>* buf, const cplx<T>* __restrict__ src, int f0) {
+    for (int idx = threadIdx.x; idx < TK * N; idx += Cfg::THREADS) {
+      const int x = idx / TK, f = idx % TK;
+      buf[f * LS + pad(x)] = src[size_t(x) * FP + f0 + f];
+    }
+  }
+  static __device__ __forceinline__ void store_tile(const cplx<T>* buf, cplx<T>* __restrict__ dst, int f0) {
+    for (int idx = threadIdx.x; idx < TK * N; idx += Cfg::THREADS) {
+      const int x = idx / TK, f = idx % TK;
+      dst[size_t(x) * FP + f0 + f] = buf[f * LS + pad(x)];
+    }
+  }
+
+  // forward x transform of the line; result in registers at kx = out_index<N,-1>
+  static __device__ __forceinline__ void forward(cplx<T> (&v)[E], cplx<T>* L, int t, const cplx<T>* __restrict__ tw,
+                                                 const cplx<T>* __restrict__ dtw) {
+    if constexpr (!DCT) {
+      fft_line<T, N, -1>(v, L, t, tw, [&](int i) { return L[pad(i)]; });
+    } else {
+      fft_line<T, N, -1>(v, L, t, tw, [&](int i) { return L[pad(i < N / 2 ? 2 * i : 2 * (N - 1 - i) + 1)]; });
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int k = out_index<N, -1>(t, b, r);
+          cplx<T> w = __ldg(&dtw[k]);
+          v[b * RL + r] = cadd<T>(cmul<T>(L[pad(k)], w), cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w)));
+        }
+    }
+  }
+
+  // inverse x transform of register values at kx = out_index<N,-1>; result
+  // written to the line in natural x order (caller syncs before reading)
+  static __device__ __forceinline__ void inverse_to_line(cplx<T> (&v)[E], cplx<T>* L, int t,
+                                                         const cplx<T>* __restrict__ tw,
+                                                         const cplx<T>* __restrict__ dtw) {
+    constexpr int RLI = radix_of<N, +1, Plan<N>::P - 1>();
+    if constexpr (!DCT) {
+      fft_regs<T, N, +1>(v, L, t, tw);
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RLI; ++b)
+#pragma unroll
+        for (int r = 0; r < RLI; ++r) L[pad(out_index<N, +1>(t, b, r))] = v[b * RLI + r];
+    } else {
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
+      __syncwarp();
+      fft_line<T, N, +1>(v, L, t, tw, [&](int i) {
+        cplx<T> a = L[pad(i)];
+        cplx<T> u = a;
+        if (i != 0) {
+          cplx<T> bb = L[pad(N - i)];
+          u = mk<T>(a.x + bb.y, a.y - bb.x);
+        }
+        cplx<T> w = __ldg(&dtw[i]);
+        w.y = -w.y;
+        return cmul<T>(u, w);
+      });
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RLI; ++b)
+#pragma unroll
+        for (int r = 0; r < RLI; ++r) {
+          const int n = out_index<N, +1>(t, b, r);
+          L[pad(n < N / 2 ? 2 * n : 2 * (N - 1 - n) + 1)] = v[b * RLI + r];
+        }
+    }
+  }
+};
+
+// Spectral multipliers of mode (kx, ky, kz) for replica epsilon ``eps``
+template <typename T>
+struct Mult {
+  T mq2, a_lin, c1, c2;
+};
+template <typename T>
+__device__ __forceinline__ Mult<T> make_mult(T qx, T qy, T qz, T eps, const PointParams& pp) {
+  Mult<T> m;
+  m.mq2 = qx * qx + qy * qy + qz * qz;
+  const T d = m.mq2 - T(pp.q0 * pp.q0);
+  const T op_sh = T(pp.alpha) * d * d;
+  m.a_lin = eps - op_sh;
+  const T h = T(0.5 * pp.dt);
+  m.c1 = T(1) + h * m.a_lin;
+  m.c2 = T(1) - h * m.a_lin;
+  return m;
+}
+
+// CNAB2 (or IMEX Euler) update of one real spectral coefficient pair
+template <typename T>
+__device__ __forceinline__ T update_one(T& w, T nh, const Mult<T>& m, const PointParams& pp) {
+  if (pp.scheme == kCNAB2) {
+    const T psi_new = (w + T(1.5 * pp.dt) * nh) / m.c2;
+    w = m.c1 * psi_new - T(0.5 * pp.dt) * nh;
+    return psi_new;
+  }
+  const T psi_new = (w + T(pp.dt) * nh) / (T(1) - T(pp.dt) * m.a_lin);
+  w = psi_new;
+  return psi_new;
+}
+
+template <typename T, int N, bool DCT, int MODE>
+__global__ void __launch_bounds__(PencilCfg<T, N, DCT>::THREADS)
+pencil_kernel(PencilArgs<T> a) {
+  using Cfg = PencilCfg<T, N, DCT>;
+  using Ops = PencilOps<T, N, DCT>;
+  constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
+  double* scratch = reinterpret_cast<double*>(smem_raw + size_t(TK) * LS * sizeof(cplx<T>));
+
+  const int f0 = blockIdx.x * TK;
+  const int rep = blockIdx.y;
+  const int line = threadIdx.x / G, t = threadIdx.x % G;
+  const int f = f0 + line;
+  cplx<T>* L = buf + line * LS;
+  const size_t plane_base = size_t(rep) * N * FP;
+  cplx<T>* wrow = a.w + (size_t(rep) * FP + f) * N;
+  const T eps = T(a.pp.eps[rep]);
+  const T scale = T(a.pp.scale);
+
+  // in-plane wavenumber indices of this line
+  int ky, kz;
+  if (DCT) {
+    ky = f / (N / 2);
+    kz = 2 * (f % (N / 2));  // the pair holds kz and kz + 1
+  } else if (f < N * (N / 2)) {
+    ky = f / (N / 2);
+    kz = f % (N / 2);
+  } else {
+    ky = f - N * (N / 2);
+    kz = N / 2;
+  }
+  const T qy = __ldg(&a.q[ky]);
+  const T qz0 = __ldg(&a.q[kz]);
+  const T qz1 = DCT ? __ldg(&a.q[kz + 1]) : T(0);
+
+  cplx<T> v[E];
+  KahanSum acc;
+  const bool want_energy = (a.flags & kFlEnergy) != 0;
+
+  if constexpr (MODE == kPencilStep) {
+    Ops::load_tile(buf, a.src + plane_base, f0);
+    __syncthreads();
+    Ops::forward(v, L, t, a.tw, a.dtw);
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int kx = out_index<N, -1>(t, b, r);
+        const T qx = __ldg(&a.q[kx]);
+        cplx<T> wv = wrow[kx];
+        const cplx<T> nh = v[b * RL + r];
+        cplx<T> pn;
+        if constexpr (!DCT) {
+          const Mult<T> m = make_mult<T>(qx, qy, qz0, eps, a.pp);
+          pn.x = update_one<T>(wv.x, nh.x, m, a.pp);
+          pn.y = update_one<T>(wv.y, nh.y, m, a.pp);
+          if (want_energy) {
+            const double d = double(a.pp.q0) * a.pp.q0 - double(m.mq2);
+            const double wgt = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
+            acc.add(wgt * d * d * (double(pn.x) * pn.x + double(pn.y) * pn.y));
+          }
+        } else {
+          const Mult<T> m0 = make_mult<T>(qx, qy, qz0, eps, a.pp);
+          const Mult<T> m1 = make_mult<T>(qx, qy, qz1, eps, a.pp);
+          pn.x = update_one<T>(wv.x, nh.x, m0, a.pp);
+          pn.y = update_one<T>(wv.y, nh.y, m1, a.pp);
+          if (want_energy) {
+            const double wxy = (kx == 0 ? 0.5 : 1.0) * (ky == 0 ? 0.5 : 1.0);
+            const double d0 = double(a.pp.q0) * a.pp.q0 - double(m0.mq2);
+            const double d1 = double(a.pp.q0) * a.pp.q0 - double(m1.mq2);
+            acc.add(wxy * ((kz == 0 ? 0.5 : 1.0) * d0 * d0 * double(pn.x) * pn.x + d1 * d1 * double(pn.y) * pn.y));
+          }
+        }
+        if (!isfinite(pn.x) || !isfinite(pn.y)) *a.nonfinite = 1;
+        wrow[kx] = wv;
+        v[b * RL + r] = cscale<T>(pn, scale);
+      }
+  } else if constexpr (MODE == kPencilEnergy) {
+    // gradient part of the energy of the current state from its partial P
+    Ops::load_tile(buf, a.src + plane_base, f0);
+    __syncthreads();
+    Ops::forward(v, L, t, a.tw, a.dtw);
+    const double inv = 1.0 / a.pp.scale;
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int kx = out_index<N, -1>(t, b, r);
+        const T qx = __ldg(&a.q[kx]);
+        const double px = double(v[b * RL + r].x) * inv, py = double(v[b * RL + r].y) * inv;
+        const double q02 = double(a.pp.q0) * a.pp.q0;
+        if constexpr (!DCT) {
+          const double d = q02 - double(qx * qx + qy * qy + qz0 * qz0);
+          const double wgt = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
+          acc.add(wgt * d * d * (px * px + py * py));
+        } else {
+          const double wxy = (kx == 0 ? 0.5 : 1.0) * (ky == 0 ? 0.5 : 1.0);
+          const double d0 = q02 - double(qx * qx + qy * qy + qz0 * qz0);
+          const double d1 = q02 - double(qx * qx + qy * qy + qz1 * qz1);
+          acc.add(wxy * ((kz == 0 ? 0.5 : 1.0) * d0 * d0 * px * px + d1 * d1 * py * py));
+        }
+      }
+  } else {  // kPencilInit: W^0 from psi^0 and N(psi^0); P^0 from psi^0
+    Ops::load_tile(buf, a.src + plane_base, f0);
+    __syncthreads();
+    Ops::forward(v, L, t, a.tw, a.dtw);
+    cplx<T> vn[E];
+    __syncthreads();
+    Ops::load_tile(buf, a.src2 + plane_base, f0);
+    __syncthreads();
+    Ops::forward(vn, L, t, a.tw, a.dtw);
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int kx = out_index<N, -1>(t, b, r);
+        const T qx = __ldg(&a.q[kx]);
+        const cplx<T> ph = v[b * RL + r], nh = vn[b * RL + r];
+        cplx<T> wv;
+        const Mult<T> m0 = make_mult<T>(qx, qy, qz0, eps, a.pp);
+        const Mult<T> m1 = DCT ? make_mult<T>(qx, qy, qz1, eps, a.pp) : m0;
+        if (a.pp.scheme == kCNAB2) {
+          wv.x = m0.c1 * ph.x - T(0.5 * a.pp.dt) * nh.x;
+          wv.y = m1.c1 * ph.y - T(0.5 * a.pp.dt) * nh.y;
+        } else {
+          wv = ph;
+        }
+        wrow[kx] = wv;
+        v[b * RL + r] = cscale<T>(ph, scale);
+      }
+  }
+
+  if constexpr (MODE != kPencilEnergy) {
+    Ops::inverse_to_line(v, L, t, a.tw, a.dtw);
+    __syncthreads();
+    Ops::store_tile(buf, a.dst + plane_base, f0);
+  }
+
+  if (want_energy && MODE != kPencilInit) {
+    const double tot = block_sum(acc.s, scratch);
+    if (threadIdx.x == 0) a.red[size_t(rep) * gridDim.x + blockIdx.x] = tot;
+  }
+}
+
+}  // namespace shb

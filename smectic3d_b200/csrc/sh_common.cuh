@@ -1,0 +1,71 @@
+// Shared definitions of the smectic3d_b200 kernels.
+#pragma once
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "fft_engine.cuh"
+
+namespace shb {
+namespace cg = cooperative_groups;
+
+enum NonlinKind : int { kQuintic = 0, kQuadCubic = 1 };
+enum SchemeKind : int { kCNAB2 = 0, kIMEXEuler = 1 };
+enum PassFlags : int { kFlPsiOut = 1, kFlL1 = 2, kFlEnergy = 4 };
+
+// Per-launch scalar parameters of the pointwise stages.
+struct PointParams {
+  double dt;
+  double beta, gamma, alpha, q0;
+  double eta_rho;       // rho * eta (Stokes)
+  double w_mid;         // pinning penalty weight
+  double inv_dz2;       // 1 / dz^2
+  double scale;         // 1/N^3 (periodic) or 1/(8 N^3) (Neumann)
+  int nonlin;           // NonlinKind
+  int scheme;           // SchemeKind
+  const double* eps;    // per-replica epsilon
+};
+
+template <typename T>
+__device__ __forceinline__ T nonlin_eval(T p, T beta, T gamma, int kind) {
+  const T p2 = p * p;
+  // beta psi^3 - gamma psi^5  (periodicFFT/pf3d.cpp:368-369)
+  if (kind == kQuintic) return p * p2 * (beta - gamma * p2);
+  // beta psi^2 - gamma psi^3
+  return p2 * (beta - gamma * p);
+}
+
+// Local part of the Lyapunov density (energyPsi.m:225-228 without the gradient
+// term, which is accumulated spectrally).
+__device__ __forceinline__ double local_density(double p, double eps, double beta, double gamma, int kind) {
+  const double p2 = p * p;
+  if (kind == kQuintic) return -0.5 * eps * p2 + p2 * p2 * (-0.25 * beta + gamma / 6.0 * p2);
+  return -0.5 * eps * p2 + p2 * p * (-beta / 3.0 + 0.25 * gamma * p);
+}
+
+// Kahan-compensated FP64 accumulator
+struct KahanSum {
+  double s = 0.0, c = 0.0;
+  __device__ __forceinline__ void add(double x) {
+    double y = x - c;
+    double t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+};
+
+// Block-wide FP64 sum; every thread returns the total.  ``scratch`` holds one
+// double per warp.
+__device__ __forceinline__ double block_sum(double v, double* scratch) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) scratch[w] = v;
+  __syncthreads();
+  const int nw = (blockDim.x + 31) >> 5;
+  double t = 0.0;
+  for (int i = 0; i < nw; ++i) t += scratch[i];
+  return t;
+}
+
+}  // namespace shb

@@ -1,0 +1,183 @@
+"""Python mirror of the reference's time-loop interface over the C-ABI.
+
+``Params`` carries the constants the reference hard-codes in main()
+(periodicFFT/pf3d.cpp:35-73, cosFFT/mesabi/cosNoAdvMorph.cpp:74-112) and
+``Solver`` runs the loop body (periodicFFT/pf3d.cpp:390-550) on the GPU.
+Arrays cross the boundary as float64 in the reference's index order
+(i, j, k with k fastest).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+
+import numpy as np
+
+from . import _lib as L
+
+
+@dataclasses.dataclass
+class Params:
+    n: int = 128
+    batch: int = 1
+    boundary: str = "periodic"       # "periodic" (R2C/C2R) or "neumann" (REDFT10/REDFT01)
+    advection: bool = False
+    nonlinearity: str = "quintic"    # beta psi^3 - gamma psi^5 (reference) | "quad_cubic"
+    scheme: str = "cnab2"            # reference CN + AB2 | "imex_euler"
+    precision: str = "fp64"          # "fp64" | "fp32"
+    l1_interval: int = 0             # 100 in the reference (periodicFFT/pf3d.cpp:489)
+    energy_trace: bool = False
+    dx: float = 2.0 * math.pi / 8.0
+    dt: float = 0.05
+    eps: float = -0.75
+    beta: float = 2.0
+    gamma: float = 1.0
+    alpha: float = 1.0
+    q0: float = 1.0
+    eta: float = 1.0
+    rho: float = 1.0
+    w_mid: float = 0.0
+    sub_sigma: float = 0.0
+    sub_z0: float = 1e-4
+    eps_per_replica: tuple | None = None
+
+    @staticmethod
+    def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":
+        """dx from points per wavelength, as the reference does: L = N 2 pi/(q0 Nw)."""
+        return Params(n=n, dx=2.0 * math.pi / (q0 * nw), q0=q0, **kw)
+
+    def to_c(self):
+        p = L.ShParams()
+        p.n, p.batch = self.n, self.batch
+        p.boundary = {"periodic": L.SH_PERIODIC, "neumann": L.SH_NEUMANN}[self.boundary]
+        p.advection = int(bool(self.advection))
+        p.nonlinearity = {"quintic": L.SH_QUINTIC, "quad_cubic": L.SH_QUAD_CUBIC}[self.nonlinearity]
+        p.scheme = {"cnab2": L.SH_CNAB2, "imex_euler": L.SH_IMEX_EULER}[self.scheme]
+        p.precision = {"fp64": L.SH_FP64, "fp32": L.SH_FP32}[self.precision]
+        p.l1_interval = self.l1_interval
+        p.energy_trace = int(bool(self.energy_trace))
+        for k in ("dx", "dt", "eps", "beta", "gamma", "alpha", "q0", "eta", "rho", "w_mid", "sub_sigma", "sub_z0"):
+            setattr(p, k, float(getattr(self, k)))
+        keep = None
+        if self.eps_per_replica is not None:
+            keep = (C.c_double * self.batch)(*[float(e) for e in self.eps_per_replica])
+            p.eps_per_replica = C.cast(keep, C.POINTER(C.c_double))
+        return p, keep
+
+
+class Solver:
+    """One GPU solver handle (all replicas of ``params.batch``)."""
+
+    def __init__(self, params: Params):
+        self.lib = L.load()
+        self.params = params
+        cp, keep = params.to_c()
+        h = C.c_void_p()
+        L.check(self.lib.sh_create(C.byref(cp), C.byref(h)), None)
+        self.h = h
+        self._keep = keep
+        n = params.n
+        self.shape = (params.batch, n, n, n) if params.batch > 1 else (n, n, n)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _chk(self, rc):
+        L.check(rc, self.h)
+
+    # -- state ---------------------------------------------------------------
+    def set_psi(self, psi: np.ndarray, layout: int = L.SH_LAYOUT_DENSE):
+        a = np.ascontiguousarray(psi, dtype=np.float64)
+        self._chk(self.lib.sh_set_psi(self.h, a.ctypes.data, layout))
+
+    def get_psi(self, layout: int = L.SH_LAYOUT_DENSE) -> np.ndarray:
+        n, b = self.params.n, self.params.batch
+        if layout == L.SH_LAYOUT_DENSE:
+            out = np.empty(self.shape, dtype=np.float64)
+        else:
+            out = np.empty((b, n, n, 2 * (n // 2 + 1)) if b > 1 else (n, n, 2 * (n // 2 + 1)), dtype=np.float64)
+        self._chk(self.lib.sh_get_psi(self.h, out.ctypes.data, layout))
+        return out
+
+    def set_psi_device(self, ptr: int):
+        self._chk(self.lib.sh_set_psi_device(self.h, C.c_void_p(ptr)))
+
+    def get_psi_device(self, ptr: int):
+        self._chk(self.lib.sh_get_psi_device(self.h, C.c_void_p(ptr)))
+
+    def step(self, nsteps: int = 1):
+        self._chk(self.lib.sh_step(self.h, int(nsteps)))
+
+    def step_async(self, nsteps: int = 1):
+        self._chk(self.lib.sh_step_async(self.h, int(nsteps)))
+
+    def run(self, psi0: np.ndarray, nsteps: int, out: np.ndarray | None = None) -> np.ndarray:
+        a = np.ascontiguousarray(psi0, dtype=np.float64)
+        if out is None:
+            out = np.empty(self.shape, dtype=np.float64)
+        self._chk(self.lib.sh_run(self.h, a.ctypes.data, int(nsteps), out.ctypes.data, L.SH_LAYOUT_DENSE))
+        return out
+
+    def synchronize(self):
+        self._chk(self.lib.sh_synchronize(self.h))
+
+    @property
+    def stream(self) -> int:
+        return self.lib.sh_stream(self.h) or 0
+
+    @property
+    def steps_taken(self) -> int:
+        return int(self.lib.sh_steps_taken(self.h))
+
+    @property
+    def kernel_launches(self) -> int:
+        c = C.c_longlong()
+        self._chk(self.lib.sh_kernel_launches(self.h, C.byref(c)))
+        return int(c.value)
+
+    # -- diagnostics -----------------------------------------------------------
+    def energy(self) -> np.ndarray:
+        out = np.empty(self.params.batch, dtype=np.float64)
+        self._chk(self.lib.sh_energy(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def energy_trace(self) -> np.ndarray:
+        cnt = C.c_int()
+        self._chk(self.lib.sh_energy_trace(self.h, None, 0, C.byref(cnt)))
+        out = np.empty((cnt.value, self.params.batch), dtype=np.float64)
+        if cnt.value:
+            self._chk(self.lib.sh_energy_trace(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), cnt.value,
+                                               C.byref(cnt)))
+        return out
+
+    def l1(self):
+        out = np.empty(self.params.batch, dtype=np.float64)
+        cnt = C.c_int()
+        self._chk(self.lib.sh_l1(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt)))
+        return out, cnt.value
+
+    def checkpoint(self) -> bytes:
+        size = C.c_size_t()
+        self._chk(self.lib.sh_checkpoint_save(self.h, None, C.byref(size)))
+        buf = (C.c_char * size.value)()
+        self._chk(self.lib.sh_checkpoint_save(self.h, buf, C.byref(size)))
+        return bytes(buf)
+
+    def restore(self, blob: bytes):
+        buf = (C.c_char * len(blob)).from_buffer_copy(blob)
+        self._chk(self.lib.sh_checkpoint_load(self.h, buf, len(blob)))

@@ -1,0 +1,112 @@
+"""Generate the golden vectors under tests/golden/ from the FP64 oracle.
+
+    python -m tests.golden.make_golden
+
+Each case stores its inputs (psi0, parameters) and the oracle's outputs, so
+the GPU parity tests compare against fixed numbers that do not depend on the
+oracle being importable or on SciPy's version.  The reference itself cannot
+be run here (it needs FFTW-MPI and MPI), so these vectors come from the
+oracle, whose pins are the analytic tests in tests/test_oracle.py.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+import os
+
+import numpy as np
+
+from oracle import sh_oracle as O
+from smectic3d_b200 import ic
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def path(name: str) -> str:
+    return os.path.join(HERE, name + ".npz")
+
+
+def _pack(p: O.Params, **arrays):
+    d = {k: np.asarray(v) for k, v in arrays.items()}
+    for f in dataclasses.fields(p):
+        v = getattr(p, f.name)
+        d["param_" + f.name] = np.asarray(v)
+    return d
+
+
+def periodic_plain():
+    n = 16
+    p = O.Params(n=n, dt=0.05)
+    psi0 = ic.noise(n, 0) + 1.2 * np.cos(np.arange(n) * p.dx)[None, None, :]
+    o = O.PeriodicOracle(psi0, p)
+    e0 = O.energy_spectral_periodic(psi0, p)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10, energy0=e0, energy=O.energy_spectral_periodic(o.psi, p))
+
+
+def periodic_lamellae_ref_ic():
+    n = 32
+    p = O.Params(n=n, dx=2 * math.pi / 16, dt=0.01, eps=-0.7)
+    psi0 = ic.pf3d_lamellae(n, p.dx)
+    o = O.PeriodicOracle(psi0, p)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10, energy=O.energy_spectral_periodic(o.psi, p))
+
+
+def periodic_imex_quadcubic():
+    n = 16
+    p = O.Params(n=n, dt=0.05, scheme="imex_euler", nonlinearity="quad_cubic", eps=0.2)
+    psi0 = ic.noise(n, 3, 0.3)
+    o = O.PeriodicOracle(psi0, p)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10)
+
+
+def periodic_penalty():
+    n = 16
+    p = O.Params(n=n, dt=0.01, w_mid=1.0)
+    psi0 = 1.3 * np.cos(np.arange(n) * p.dx)[None, None, :] + ic.noise(n, 4, 0.2)
+    o = O.PeriodicOracle(psi0, p)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10)
+
+
+def neumann_hyperboloid():
+    n = 16
+    p = O.Params(n=n, dt=0.05)
+    psi0 = ic.hyperboloid(n, p.dx, r0_cells=5.0, seed=5)
+    o = O.NeumannOracle(psi0, p)
+    e0 = O.energy_spectral_neumann(psi0, p)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10, energy0=e0, energy=O.energy_spectral_neumann(o.psi, p))
+
+
+def neumann_l1():
+    n = 32
+    p = O.Params(n=n, dt=0.05, eps=-0.7)
+    psi0 = ic.cos_bottom_hyperboloid(n, p.dx)
+    o = O.NeumannOracle(psi0, p)
+    o.run(19)
+    prev = o.psi.copy()
+    o.step()
+    return _pack(p, psi0=psi0, psi=o.psi, steps=20, l1=O.l1_monitor(o.psi, prev, p.dt))
+
+
+CASES = {
+    "periodic_plain_16": periodic_plain,
+    "periodic_lamellae_32": periodic_lamellae_ref_ic,
+    "periodic_imex_quadcubic_16": periodic_imex_quadcubic,
+    "periodic_penalty_16": periodic_penalty,
+    "neumann_hyperboloid_16": neumann_hyperboloid,
+    "neumann_l1_32": neumann_l1,
+}
+
+
+def main():
+    for name, fn in CASES.items():
+        np.savez_compressed(path(name), **fn())
+        print("wrote", path(name))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""CPU checks of the C-ABI library: it loads, exports every entry point the
+header declares, agrees with the ctypes mirror on struct layout, and rejects
+bad parameters before touching the GPU."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from smectic3d_b200 import _lib as L
+from smectic3d_b200.solver import Params
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "smectic_b200.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    return sorted(set(re.findall(r"^\s*(?:int|void\*|long long|const char\*)\s+(sh_\w+)\s*\(", src, re.M)))
+
+
+def test_header_declares_what_binding_knows():
+    assert set(declared_symbols()) == set(L.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version_string(lib):
+    assert b"sm_100a" in lib.sh_version()
+
+
+def test_params_struct_layout_matches_header():
+    prog = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "smectic_b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\n", sizeof(sh_params), offsetof(sh_params, dx), offsetof(sh_params, w_mid),
+         offsetof(sh_params, sub_z0), offsetof(sh_params, eps_per_replica));
+  return 0;
+}
+"""
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(prog)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    got = [int(v) for v in out]
+    P = L.ShParams
+    assert got == [C.sizeof(P), P.dx.offset, P.w_mid.offset, P.sub_z0.offset, P.eps_per_replica.offset]
+
+
+def test_default_params(lib):
+    p = L.ShParams()
+    assert lib.sh_default_params(C.byref(p)) == L.SH_OK
+    assert p.n == 128 and p.batch == 1 and p.boundary == L.SH_PERIODIC
+    assert p.eps == -0.75 and p.beta == 2.0 and p.gamma == 1.0 and p.q0 == 1.0
+    assert abs(p.dx - 2 * 3.141592653589793 / 8) < 1e-15 and p.dt == 0.05
+
+
+@pytest.mark.parametrize(
+    "field,value,code",
+    [
+        ("n", 48, L.SH_EUNSUPPORTED),
+        ("n", 1024, L.SH_EUNSUPPORTED),
+        ("batch", 0, L.SH_EINVAL),
+        ("boundary", 7, L.SH_EINVAL),
+        ("precision", 3, L.SH_EINVAL),
+        ("scheme", 9, L.SH_EINVAL),
+        ("dt", -1.0, L.SH_EINVAL),
+        ("dx", 0.0, L.SH_EINVAL),
+        ("l1_interval", -2, L.SH_EINVAL),
+    ],
+)
+def test_create_rejects_bad_params(lib, field, value, code):
+    p = L.ShParams()
+    lib.sh_default_params(C.byref(p))
+    setattr(p, field, value)
+    h = C.c_void_p()
+    assert lib.sh_create(C.byref(p), C.byref(h)) == code
+    assert not h.value
+    assert lib.sh_last_error(None)
+
+
+def test_create_rejects_neumann_advection(lib):
+    p = L.ShParams()
+    lib.sh_default_params(C.byref(p))
+    p.boundary = L.SH_NEUMANN
+    p.advection = 1
+    h = C.c_void_p()
+    assert lib.sh_create(C.byref(p), C.byref(h)) == L.SH_EINVAL
+
+
+def test_null_arguments(lib):
+    assert lib.sh_create(None, None) == L.SH_EINVAL
+    assert lib.sh_destroy(None) == L.SH_EINVAL
+    assert lib.sh_step(None, 1) == L.SH_EINVAL
+    assert lib.sh_default_params(None) == L.SH_EINVAL
+
+
+def test_python_params_mapping():
+    p = Params(n=64, boundary="neumann", precision="fp32", scheme="imex_euler", nonlinearity="quad_cubic",
+               batch=3, eps_per_replica=(-0.9, -0.7, -0.5))
+    cp, keep = p.to_c()
+    assert (cp.n, cp.boundary, cp.precision, cp.scheme, cp.nonlinearity) == (64, 1, 1, 1, 1)
+    assert [cp.eps_per_replica[i] for i in range(3)] == [-0.9, -0.7, -0.5]
+    fn = Params.from_nw(256, 16)
+    assert abs(fn.dx - 2 * 3.141592653589793 / 16) < 1e-15

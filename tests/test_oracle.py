@@ -1,0 +1,214 @@
+"""Pins of the FP64 oracle (CPU only).
+
+The reference ships no tests or golden outputs and cannot be built here, so the
+oracle is pinned to analytic known-answer tests of the reference's algorithm:
+FFTW's transform conventions, the exact CNAB2 growth factor of grid modes
+(the pf3dVal validation, periodicFFT/pf3dVal.cpp:214-331, restricted to
+grid-commensurate wavenumbers), the lamellar amplitude of the reference ICs,
+Lyapunov decrease, the Stokes projector and the surfTrack crossing.
+"""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+import scipy.fft as sfft
+
+from oracle import sh_oracle as O
+
+
+def test_wavenumbers_follow_reference_formula():
+    n, dx = 16, 2 * math.pi / 8
+    q = O.kvec_periodic(n, dx)
+    # periodicFFT/pf3d.cpp:176-182 (Vqy form, explicit Nyquist +pi/dy)
+    ref = np.zeros(n)
+    ref[n // 2] = math.pi / dx
+    for j in range(1, n // 2):
+        ref[j] = 2 * math.pi * j / (dx * n)
+        ref[n // 2 + j] = -(n // 2 - j) * 2 * math.pi / (dx * n)
+    assert np.allclose(q, ref, rtol=0, atol=1e-15)
+    qd = O.kvec_dct(n, dx)
+    assert np.allclose(qd, math.pi * np.arange(n) / (dx * n))
+
+
+def test_fftw_scale_conventions():
+    rng = np.random.default_rng(0)
+    a = rng.standard_normal((8, 8, 8))
+    # unnormalised r2c then c2r multiplies by N^3 (the reference scales by 1/NG)
+    assert np.allclose(O.c2r(O.r2c(a), 8), a * 512, atol=1e-10)
+    # REDFT10 then REDFT01 multiplies by (2N)^3 (cosNoAdvMorph scale 0.125/N^3)
+    assert np.allclose(O.idct3d(O.dct3d(a)), a * 8 * 512, atol=1e-9)
+    # REDFT10 definition: Y[k] = 2 sum x[n] cos(pi (2n+1) k / 2N)
+    x = rng.standard_normal(8)
+    k = np.arange(8)[:, None]
+    nn = np.arange(8)[None, :]
+    y = 2 * (x[None, :] * np.cos(np.pi * (2 * nn + 1) * k / 16)).sum(1)
+    assert np.allclose(sfft.dct(x, type=2), y)
+    # REDFT01: Y[n] = X[0] + 2 sum_{k>0} X[k] cos(pi k (2n+1) / 2N)
+    y3 = x[0] + 2 * (x[None, 1:] * np.cos(np.pi * np.arange(1, 8)[None, :] * (2 * np.arange(8)[:, None] + 1) / 16)).sum(1)
+    assert np.allclose(sfft.dct(x, type=3), y3)
+
+
+def test_c2r_semantics_non_hermitian():
+    """FFTW c2r: complex inverse over x, y, then the real part on kz=0, N/2."""
+    rng = np.random.default_rng(1)
+    n = 8
+    a = rng.standard_normal((n, n, n // 2 + 1)) + 1j * rng.standard_normal((n, n, n // 2 + 1))
+    g = np.fft.ifft(np.fft.ifft(a, axis=0), axis=1) * n * n
+    full = np.zeros((n, n, n), complex)
+    full[:, :, : n // 2 + 1] = g
+    full[:, :, 0] = g[:, :, 0].real
+    full[:, :, n // 2] = g[:, :, n // 2].real
+    for kz in range(n // 2 + 1, n):
+        full[:, :, kz] = np.conj(g[:, :, n - kz])
+    ref = np.fft.ifft(full, axis=2).real * n
+    assert np.allclose(O.c2r(a, n), ref, atol=1e-12)
+
+
+@pytest.mark.parametrize("boundary", ["periodic", "neumann"])
+def test_linear_growth_factor_kat(boundary):
+    """beta = gamma = 0: one CNAB2 step multiplies mode q by (1+dt a/2)/(1-dt a/2),
+    a = eps - (q^2 - q0^2)^2 -- the pf3dVal validation on grid modes."""
+    n = 32
+    p = O.Params(n=n, dt=0.1, eps=0.1, beta=0.0, gamma=0.0)
+    kv = O.kvec_periodic(n, p.dx) if boundary == "periodic" else O.kvec_dct(n, p.dx)
+    z = np.arange(n)
+    for m in (1, 3, 4, 5, 8):
+        q = kv[m]
+        if boundary == "periodic":
+            prof = np.cos(2 * math.pi * m * z / n)
+        else:
+            prof = np.cos(math.pi * m * (z + 0.5) / n)
+        psi0 = 1e-4 * np.broadcast_to(prof, (n, n, n)).copy()
+        orc = (O.PeriodicOracle if boundary == "periodic" else O.NeumannOracle)(psi0, p)
+        a = p.eps - (q * q - p.q0 ** 2) ** 2
+        g = (1 + p.dt * a / 2) / (1 - p.dt * a / 2)
+        for s in range(1, 4):
+            orc.step()
+            assert np.allclose(orc.psi, g ** s * psi0, rtol=1e-11, atol=1e-18)
+
+
+def test_lamellar_amplitude_matches_reference_ic():
+    """psi = A cos(q0 z) at eps=-0.7 relaxes to the reference amplitude 1.328
+    (cosFFT/comet/cosNoAdvMorph.cpp:322); one-mode estimate 1.3288."""
+    n = 16
+    p = O.Params(n=n, dt=0.1, eps=-0.7)
+    z = np.arange(n) * p.dx
+    psi0 = np.broadcast_to(1.0 * np.cos(z), (n, n, n)).copy()
+    orc = O.PeriodicOracle(psi0, p)
+    orc.run(600)
+    amp = orc.psi.max()
+    assert abs(amp - 1.328) < 0.03
+    psi0 = np.broadcast_to(0.5 * np.cos(z), (n, n, n)).copy()  # below threshold decays
+    orc = O.PeriodicOracle(psi0, p)
+    orc.run(300)
+    assert np.abs(orc.psi).max() < 0.05
+
+
+@pytest.mark.parametrize("boundary", ["periodic", "neumann"])
+def test_lyapunov_decrease(boundary):
+    n = 16
+    p = O.Params(n=n, dt=0.02, eps=-0.7)
+    psi0 = 1.3 * np.cos(np.arange(n) * p.dx)[None, None, :] + np.random.default_rng(2).uniform(-0.3, 0.3, (n, n, n))
+    orc = (O.PeriodicOracle if boundary == "periodic" else O.NeumannOracle)(psi0, p)
+    efun = O.energy_spectral_periodic if boundary == "periodic" else O.energy_spectral_neumann
+    e = [efun(orc.psi, p)]
+    for _ in range(40):
+        orc.step()
+        e.append(efun(orc.psi, p))
+    assert all(e[i + 1] <= e[i] + 1e-9 * abs(e[i]) for i in range(len(e) - 1))
+
+
+def test_energy_forms_agree_on_smooth_field():
+    """FD+trapz (energyPsi.m) and spectral forms agree as the grid resolves psi."""
+    n = 64
+    p = O.Params(n=n, dx=2 * math.pi / 32, eps=-0.7)
+    z = np.arange(n) * p.dx
+    psi = np.broadcast_to(1.3 * np.cos(z), (n, n, n)).copy()
+    es = O.energy_spectral_periodic(psi, p)
+    ef = O.energy_fd_trapz(psi, p)
+    # trapz drops half of the two end planes of a periodic sum; FD Laplacian O(dx^2)
+    assert abs(es - ef) / abs(es) < 0.05
+
+
+def test_stokes_projector_identities():
+    n = 16
+    p = O.Params(n=n)
+    rng = np.random.default_rng(3)
+    psi = rng.uniform(-1, 1, (n, n, n))
+    orc = O.PeriodicOracle(psi, p, advect=True)
+    (ux, uy, uz), grads, lpsi = orc.velocity(O.r2c(psi))
+    uq = [O.r2c(u) for u in (ux, uy, uz)]
+    div = orc.qx * uq[0] + orc.qy * uq[1] + orc.qz * uq[2]
+    # q . u = 0 away from the Nyquist planes (where q_{N/2} = +pi/dx breaks the
+    # Hermitian pairing of the C2R/R2C round trip)
+    inner = div[1:n // 2, 1:n // 2, 1:n // 2]
+    assert np.abs(inner).max() < 1e-9 * max(1.0, np.abs(uq[0]).max())
+    assert abs(uq[0][0, 0, 0]) < 1e-12 and abs(uq[2][0, 0, 0]) < 1e-12
+    # single-mode forcing: u = S_perp / (rho eta q^2)
+    s = np.zeros((n, n, n))
+    x = np.arange(n) * p.dx
+    s = np.broadcast_to(np.cos(2 * math.pi * 2 * x / (n * p.dx))[None, None, :], (n, n, n)).copy()
+    sq = O.r2c(s)
+    zero = np.zeros_like(sq)
+    dot = orc.qx * zero + orc.qy * sq + orc.qz * zero
+    uy = O.c2r(orc.scale * orc.cm1 * (sq - orc.cm2y * dot), n)
+    # forcing along y varying along z is transverse: u_y = S / q^2
+    q = 2 * math.pi * 2 / (n * p.dx)
+    assert np.allclose(uy, s / q ** 2, atol=1e-12)
+
+
+def test_surface_scan_planar_front():
+    """psi = cos(q0 (z - z0)) + tilt-free: the crossing sits at the first
+    descending zero after psi > 0.1, H = K = 0."""
+    n = 32
+    p = O.Params(n=n, dt=0.01, beta=0.0, gamma=0.0, eps=0.0)
+    z = np.arange(n) * p.dx
+    psi0 = np.broadcast_to(np.cos(z - 0.3), (n, n, n)).copy()
+    orc = O.PeriodicOracle(psi0, p)
+    orc.step()
+    fields = orc.surface_fields()
+    zi, vn, hh, kk = O.surface_scan(orc.psi, *fields)
+    col = orc.psi[0, 0]
+    k = next(k for k in range(1, n) if col[k] < 0 and any(col[:k] > 0.1))
+    assert (zi == k).all()
+    assert np.abs(hh).max() < 1e-10 and np.abs(kk).max() < 1e-10
+    assert np.isfinite(vn).all()
+
+
+def test_adjoint_matches_finite_differences():
+    n = 8
+    p = O.Params(n=n, dt=0.05)
+    rng = np.random.default_rng(4)
+    psi0 = rng.uniform(-1.2, 1.2, (n, n, n))
+    tgt = 0.5 * np.broadcast_to(np.cos(1.05 * np.arange(n) * p.dx), (n, n, n))
+    steps = 6
+    loss, ge, gq, gpsi = O.adjoint_gradients_periodic(psi0, p, steps, tgt)
+
+    def lossf(pp, ps):
+        o = O.PeriodicOracle(ps, pp)
+        o.run(steps)
+        return 0.5 * ((o.psi - tgt) ** 2).sum()
+
+    h = 1e-5
+    fe = (lossf(dataclasses.replace(p, eps=p.eps + h), psi0) - lossf(dataclasses.replace(p, eps=p.eps - h), psi0)) / (2 * h)
+    fq = (lossf(dataclasses.replace(p, q0=p.q0 + h), psi0) - lossf(dataclasses.replace(p, q0=p.q0 - h), psi0)) / (2 * h)
+    d = np.zeros_like(psi0)
+    d[1, 2, 3] = 1
+    fp = (lossf(p, psi0 + h * d) - lossf(p, psi0 - h * d)) / (2 * h)
+    assert abs(ge - fe) <= 1e-6 * max(1, abs(fe))
+    assert abs(gq - fq) <= 1e-6 * max(1, abs(fq))
+    assert abs(gpsi[1, 2, 3] - fp) <= 1e-6 * max(1, abs(fp))
+
+
+def test_golden_fixtures_reproduce():
+    """The committed golden vectors (tests/golden) are what the oracle computes."""
+    from tests.golden import make_golden as G
+    for name, fn in G.CASES.items():
+        ref = np.load(G.path(name))
+        got = fn()
+        for k in ref.files:
+            if ref[k].dtype.kind in "fc":
+                assert np.allclose(got[k], ref[k], rtol=1e-12, atol=1e-14), (name, k)
+            else:
+                assert (np.asarray(got[k]) == ref[k]).all(), (name, k)
