@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Headline benchmark: 256^3 Swift-Hohenberg steps/s on one B200 (FP32 path,
+with the FP64 path timed beside it), in the configuration the metric is quoted
+on: the Neumann (REDFT10/REDFT01) solver of cosNoAdvMorph at 256^3,
+eps=-0.75, beta=2, gamma=1, q0=1, dx=2 pi/8, dt=0.05, hyperboloid initial
+condition 0.5 cos(q0 s) + 1e-3 U(-1,1) (seeded synthetic input).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload neumann256|periodic256|periodic128|batch64]
+
+A step is one time step of every domain the job integrates.  With N GPUs each
+rank integrates its own domain (replicas only: the path does not shard), and
+``value`` is the total steps of all ranks divided by the slowest rank's
+device time.  One JSON line is printed by rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "256³ SH steps/s: FP32 vs FP64 GPU @ψ rel err≤1e-5; adjoint/forward time ratio"
+L2_BYTES = 126 * 2 ** 20
+
+WORKLOADS = {
+    # name: (boundary, n, batch, precision, ic)
+    "neumann256": ("neumann", 256, 1, "fp32", "hyperboloid"),
+    "periodic256": ("periodic", 256, 1, "fp32", "noise"),
+    "periodic128": ("periodic", 128, 1, "fp64", "noise"),
+    "batch64": ("periodic", 64, 64, "fp32", "noise"),
+}
+
+
+def make_ic(kind, n, batch, dx, seed=0):
+    from smectic3d_b200 import ic
+    if kind == "hyperboloid":
+        a = ic.hyperboloid(n, dx, seed=seed)
+    else:
+        a = ic.noise(n, seed) if batch == 1 else ic.noise_batch(n, range(seed, seed + batch))
+    return a
+
+
+def params_for(workload, precision=None):
+    import numpy as np
+    import smectic3d_b200 as S
+    bnd, n, batch, prec, _ = WORKLOADS[workload]
+    kw = {}
+    if batch > 1:
+        kw["eps_per_replica"] = tuple(np.linspace(-0.9, -0.5, batch))
+    return S.Params(n=n, batch=batch, boundary=bnd, precision=precision or prec, dt=0.05, eps=-0.75, **kw)
+
+
+def algorithmic_bytes(boundary, n, batch, precision):
+    """Bytes one launch of each pass must move (read its inputs once, write
+    its outputs once): pencil reads N-partial + W, writes W + psi-partial;
+    plane reads the psi-partial, writes the N-partial."""
+    s = 4 if precision == "fp32" else 8
+    if boundary == "periodic":
+        field = 2 * s * n * n * (n // 2 + 1)     # H: half spectrum
+    else:
+        field = s * n ** 3                        # R: real field
+    return {"pencil": 4 * field * batch, "plane": 2 * field * batch, "field": field * batch}
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_record(kernel_key):
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(path):
+        return None
+    return json.load(open(path)).get(kernel_key)
+
+
+def timed_steps(solver, k, torch, dist):
+    ext = torch.cuda.ExternalStream(solver.stream)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    solver.synchronize()
+    torch.cuda.synchronize()
+    start.record(ext)
+    solver.step_async(k)
+    end.record(ext)
+    end.synchronize()
+    solver.synchronize()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if dist is not None:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def run_ours(args, rank, world, local_rank, dist):
+    import numpy as np
+    import torch
+
+    import smectic3d_b200 as S
+
+    torch.cuda.set_device(local_rank)
+    bnd, n, batch, prec, ick = WORKLOADS[args.workload]
+    p32 = params_for(args.workload)
+    psi0 = make_ic(ick, n, batch, p32.dx, seed=rank)
+    k, w = args.steps, args.warmup
+
+    # ---- device-resident timing of the headline precision -----------------
+    s32 = S.Solver(p32)
+    s32.set_psi(psi0)
+    s32.step(w)
+    l0 = s32.kernel_launches
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ms = timed_steps(s32, k, torch, dist)
+    clk = clocks.stop()
+    launches = s32.kernel_launches - l0
+    value = world * k / (ms / 1e3)
+
+    # ---- the other precision (ratio and accuracy of the FP32 path) ---------
+    other = "fp64" if prec == "fp32" else "fp32"
+    s64 = S.Solver(params_for(args.workload, other))
+    s64.set_psi(psi0)
+    s64.step(w)
+    ms64 = timed_steps(s64, k, torch, dist)
+    a32 = s32.get_psi()
+    a64 = s64.get_psi()
+    rel_err = float(np.linalg.norm(a32 - a64) / max(np.linalg.norm(a64 if prec == "fp32" else a32), 1e-300))
+    s64.close()
+
+    # ---- per-pass device times (roofline of the dominant kernel) -----------
+    nprof = max(10, min(200, k // 10))
+    ms_pencil, ms_plane = s32.profile_steps(nprof)
+    s32.close()
+    ab = algorithmic_bytes(bnd, n, batch, prec)
+    per = {"pencil": ms_pencil / nprof, "plane": ms_plane / nprof}
+    dom = max(per, key=per.get)
+    peak, peak_kind = peaks()
+    achieved = ab[dom] / (per[dom] / 1e3) / 1e9
+    tr = traffic_record(f"{dom}/{args.workload}/{prec}")
+
+    # ---- end to end through the public API with host buffers ---------------
+    pe = params_for(args.workload)
+    pe.l1_interval = 100
+    se = S.Solver(pe)
+    nbytes = psi0.size * 8
+    hp_in, hp_out = C.c_void_p(), C.c_void_p()
+    S.load_library().sh_host_alloc(nbytes, C.byref(hp_in))
+    S.load_library().sh_host_alloc(nbytes, C.byref(hp_out))
+    host_in = np.ctypeslib.as_array((C.c_double * psi0.size).from_address(hp_in.value)).reshape(psi0.shape)
+    host_out = np.ctypeslib.as_array((C.c_double * psi0.size).from_address(hp_out.value)).reshape(psi0.shape)
+    host_in[...] = psi0
+    se.run(host_in, w, host_out)  # warm
+    if dist is not None:
+        dist.barrier()
+    t0 = time.perf_counter()
+    se.run(host_in, k, host_out)
+    t1 = time.perf_counter()
+    e2e_s = t1 - t0
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    se.close()
+    S.load_library().sh_host_free(hp_in)
+    S.load_library().sh_host_free(hp_out)
+    e2e = {"value": world * k / e2e_s, "unit": "steps/s",
+           "h2d_bytes_per_step": nbytes / k, "d2h_bytes_per_step": (nbytes + 8 * batch * (k // 100) + 4) / k,
+           "api": "smectic3d_b200.Solver.run -> sh_run (pinned host psi in, K steps with the L1 monitor every 100, psi out)"}
+
+    if rank != 0:
+        return None
+    cpu = cpu_baseline(args.workload, budget_s=args.cpu_seconds) if world == 1 else None
+    field_mb = ab["field"] / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": k, "warmup": w,
+        "ms_per_step": ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32" if prec == "fp32" else "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {bnd} {n}^3 x{batch}, {WORKLOADS[args.workload][4]} IC, dt=0.05, "
+                               f"eps=-0.75, beta=2, gamma=1, q0=1, dx=2pi/8",
+                   "precision": prec, "parallelism": f"replicas x{world}",
+                   "l2": f"inputs larger than L2: working set {3 * field_mb:.0f} MB > 126 MB, no flush"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": ab[dom], "avg_launch_ms": per[dom],
+                     "traffic": (tr["bytes_per_launch"] if tr else None),
+                     "step_frac": (ab["pencil"] + ab["plane"]) / (ms / k / 1e3) / 1e9 / peak,
+                     "pass_ms": per},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "other_precision": {"precision": other, "value": world * k / (ms64 / 1e3), "ms_per_step": ms64 / k,
+                            "speedup_fp32_over_fp64": (ms64 / ms) if prec == "fp32" else (ms / ms64),
+                            "rel_err_fp32_vs_fp64": rel_err, "after_steps": w + k},
+        "adjoint_forward_ratio": None,
+    }
+    return line
+
+
+# ---------------------------------------------------------------------------
+# CPU legs: the oracle port (the reference itself needs FFTW-MPI + MPI)
+# ---------------------------------------------------------------------------
+def _oracle_solver(workload):
+    from oracle import sh_oracle as O
+    bnd, n, batch, _, ick = WORKLOADS[workload]
+    p = params_for(workload)
+    op = O.Params(n=n, dx=p.dx, dt=p.dt, eps=p.eps, beta=p.beta, gamma=p.gamma, alpha=p.alpha, q0=p.q0)
+    psi0 = make_ic(ick, n, 1, p.dx)
+    cls = O.PeriodicOracle if bnd == "periodic" else O.NeumannOracle
+    return cls(psi0, op), batch
+
+
+def cpu_baseline(workload, budget_s=20.0, max_steps=None):
+    orc, batch = _oracle_solver(workload)
+    orc.step()  # warm
+    t0 = time.perf_counter()
+    steps = 0
+    while True:
+        orc.step()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s or (max_steps and steps >= max_steps):
+            break
+    n = orc.n
+    # a step of the workload advances all `batch` domains: one oracle domain-step is 1/batch of it
+    return {"value": steps / el / batch, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{steps} oracle steps of one {n}^3 FP64 domain (SciPy pocketfft, workers={os.cpu_count()}) "
+                      f"in {el:.1f} s" + (f", scaled by 1/{batch} domains" if batch > 1 else "")}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    k = min(args.steps, 30)
+    w = min(args.warmup, 1)
+    orc, batch = _oracle_solver(args.workload)
+    for _ in range(w):
+        orc.step()
+    t0 = time.perf_counter()
+    for _ in range(k):
+        orc.step()
+    el = time.perf_counter() - t0
+    v = k / el / batch
+    bnd, n, _, prec, _ = WORKLOADS[args.workload]
+    cb = {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
+          "sample": f"{k} steps (of the requested {args.steps}) of one {n}^3 FP64 domain, oracle port on "
+                    f"SciPy pocketfft with workers={os.cpu_count()}; the reference needs FFTW-MPI + MPI, absent here"}
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": k,
+            "warmup": w, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: {bnd} {n}^3 x{batch}", "precision": "fp64 (CPU)"},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="neumann256", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        line = run_reference(args, rank)
+        if line is not None:
+            print(json.dumps(line), flush=True)
+        return
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist_mod
+        torch.cuda.set_device(local_rank)
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist = dist_mod
+    try:
+        line = run_ours(args, rank, world, local_rank, dist)
+    finally:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

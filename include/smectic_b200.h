@@ -60,7 +60,7 @@ typedef struct sh_params {
   int precision;     /* SH_FP64 / SH_FP32                                    */
   int l1_interval;   /* steps between L1 evaluations (pf3d.cpp:489: 100); 0 = off */
   int energy_trace;  /* 1: record the energy of every new state              */
-  int reserved;
+  int variant;       /* kernel shape override (0 = default; see sh_variants)  */
   double dx, dt, eps, beta, gamma, alpha, q0, eta, rho;
   double w_mid;      /* pinning penalty weight (periodicFFT/pf3dMorph.cpp:102) */
   double sub_sigma;  /* substrate penalty sigma (cosFFT/comet/cosNoAdvMorph.cpp:67-74) */
@@ -122,6 +122,10 @@ int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes);
 /* Pinned host memory for fast host<->device copies. */
 int sh_host_alloc(size_t bytes, void** out);
 int sh_host_free(void* p);
+
+/* Run `nsteps` steps timing every kernel launch with CUDA events; returns
+ * the summed device milliseconds of the pencil (x) and plane (y,z) passes. */
+int sh_profile_steps(sh_handle* h, int nsteps, double* ms_pencil, double* ms_plane);
 
 int sh_synchronize(sh_handle* h);
 void* sh_stream(sh_handle* h);               /* the handle's cudaStream_t */

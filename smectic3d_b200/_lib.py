@@ -23,7 +23,7 @@ EXPORTS = (
     "sh_default_params", "sh_create", "sh_destroy", "sh_set_psi", "sh_set_psi_device", "sh_get_psi",
     "sh_get_psi_device", "sh_step", "sh_step_async", "sh_run", "sh_energy", "sh_energy_trace", "sh_l1",
     "sh_surface_step", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
-    "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
+    "sh_profile_steps", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
 )
 
 
@@ -31,7 +31,7 @@ class ShParams(C.Structure):
     _fields_ = [
         ("n", C.c_int), ("batch", C.c_int), ("boundary", C.c_int), ("advection", C.c_int),
         ("nonlinearity", C.c_int), ("scheme", C.c_int), ("precision", C.c_int), ("l1_interval", C.c_int),
-        ("energy_trace", C.c_int), ("reserved", C.c_int),
+        ("energy_trace", C.c_int), ("variant", C.c_int),
         ("dx", C.c_double), ("dt", C.c_double), ("eps", C.c_double), ("beta", C.c_double),
         ("gamma", C.c_double), ("alpha", C.c_double), ("q0", C.c_double), ("eta", C.c_double),
         ("rho", C.c_double), ("w_mid", C.c_double), ("sub_sigma", C.c_double), ("sub_z0", C.c_double),
@@ -76,6 +76,7 @@ def load() -> C.CDLL:
         "sh_checkpoint_load": (C.c_int, [vp, vp, C.c_size_t]),
         "sh_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
         "sh_host_free": (C.c_int, [vp]),
+        "sh_profile_steps": (C.c_int, [vp, C.c_int, dp, dp]),
         "sh_synchronize": (C.c_int, [vp]),
         "sh_stream": (vp, [vp]),
         "sh_steps_taken": (C.c_longlong, [vp]),

@@ -77,6 +77,75 @@ __host__ __device__ constexpr int ns_of() {
     ns *= (DIR < 0 ? Plan<N>::R[s] : Plan<N>::R[Plan<N>::P - 1 - s]);
   return ns;
 }
+// Twiddles live in a pass-major table per direction: pass s >= 1 owns
+// (R_s - 1) * NS_s entries, entry (r - 1) * NS_s + jm = w_N^{+-jm r N/(NS_s R_s)}
+// (the inverse table holds the conjugates), so the G threads of a group read
+// consecutive entries.
+template <int N, int DIR, int S>
+__host__ __device__ constexpr int tw_offset() {
+  int off = 0;
+  for (int s = 1; s < S; ++s) {
+    int ns = 1;
+    for (int u = 0; u < s; ++u) ns *= (DIR < 0 ? Plan<N>::R[u] : Plan<N>::R[Plan<N>::P - 1 - u]);
+    const int r = DIR < 0 ? Plan<N>::R[s] : Plan<N>::R[Plan<N>::P - 1 - s];
+    off += (r - 1) * ns;
+  }
+  return off;
+}
+template <int N, int DIR>
+__host__ __device__ constexpr int tw_size() { return tw_offset<N, DIR, Plan<N>::P>(); }
+
+// Twiddle tables of one transform length, staged in shared memory per CTA:
+// forward pass table, inverse pass table, quarter-wave exp(-i pi k / 2N).
+template <typename T>
+struct TwTables {
+  const cplx<T>* f;
+  const cplx<T>* i;
+  const cplx<T>* d;
+};
+// total entries of the device table [forward | inverse | quarter-wave]
+template <int N>
+__host__ __device__ constexpr int tw_total() { return tw_size<N, -1>() + tw_size<N, +1>() + N; }
+
+// Build the device table on the host (long double trigonometry).
+template <typename T, int N, class Vec>
+void host_twiddles(Vec& out) {
+  const long double pi = 3.141592653589793238462643383279502884L;
+  out.resize(tw_total<N>());
+  int o = 0;
+  for (int dir = -1; dir <= 1; dir += 2) {
+    for (int s = 1; s < Plan<N>::P; ++s) {
+      int ns = 1;
+      for (int u = 0; u < s; ++u) ns *= (dir < 0 ? Plan<N>::R[u] : Plan<N>::R[Plan<N>::P - 1 - u]);
+      const int r_s = dir < 0 ? Plan<N>::R[s] : Plan<N>::R[Plan<N>::P - 1 - s];
+      for (int r = 1; r < r_s; ++r)
+        for (int jm = 0; jm < ns; ++jm) {
+          const long double a = dir * 2.0L * pi * (long double)(jm * r) / (long double)(ns * r_s);
+          out[o].x = T(cosl(a));
+          out[o].y = T(sinl(a));
+          ++o;
+        }
+    }
+  }
+  for (int k = 0; k < N; ++k) {
+    const long double b = -pi * k / (2.0L * N);
+    out[o].x = T(cosl(b));
+    out[o].y = T(sinl(b));
+    ++o;
+  }
+}
+
+// copy the device table into shared memory (caller syncs)
+template <typename T, int N>
+__device__ __forceinline__ TwTables<T> stage_twiddles(cplx<T>* smem, const cplx<T>* __restrict__ g, int tid, int nthr) {
+  for (int i = tid; i < tw_total<N>(); i += nthr) smem[i] = __ldg(&g[i]);
+  TwTables<T> t;
+  t.f = smem;
+  t.i = smem + tw_size<N, -1>();
+  t.d = smem + tw_size<N, -1>() + tw_size<N, +1>();
+  return t;
+}
+
 // element index held in register slot (b*R + r) after the last pass of
 // direction DIR (equivalently: loaded in that slot by the first pass of -DIR)
 template <int N, int DIR>
@@ -186,12 +255,9 @@ __device__ __forceinline__ void pass_compute(cplx<T> (&v)[Plan<N>::E], int t, co
   for (int b = 0; b < NB; ++b) {
     if constexpr (NS > 1) {
       const int jm = (t + G * b) & (NS - 1);
+      constexpr int OFF = tw_offset<N, DIR, S>();
 #pragma unroll
-      for (int r = 1; r < R; ++r) {
-        cplx<T> w = __ldg(&tw[jm * r * (N / (NS * R))]);
-        if (DIR > 0) w.y = -w.y;
-        v[b * R + r] = cmul<T>(v[b * R + r], w);
-      }
+      for (int r = 1; r < R; ++r) v[b * R + r] = cmul<T>(v[b * R + r], tw[OFF + (r - 1) * NS + jm]);
     }
     DFT<T, R, DIR>::run(&v[b * R]);
   }
@@ -240,6 +306,7 @@ __device__ __forceinline__ void passes_from(cplx<T>* line, cplx<T> (&v)[Plan<N>:
 
 // Full transform.  The first pass reads element i through ld(i); the result of
 // the last pass stays in v (element out_index<N,DIR>(t,b,r) in slot b*R+r).
+// ``tw`` is the pass-major twiddle table of direction DIR (shared memory).
 // ``line`` is scratch for the intermediate passes (it may be the line that ld
 // reads: every read of the first pass happens before the first store).
 template <typename T, int N, int DIR, class Loader>

@@ -31,7 +31,9 @@ struct PencilCfg {
   static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
   static constexpr int TILES = FP / TK;
   static constexpr int RL = radix_of<N, -1, Plan<N>::P - 1>();
-  static constexpr size_t SMEM = size_t(TK) * LS * sizeof(cplx<T>) + 64 * sizeof(double);
+  static constexpr size_t TW_OFF = size_t(TK) * LS * sizeof(cplx<T>);
+  static constexpr size_t RED_OFF = TW_OFF + size_t(tw_total<N>()) * sizeof(cplx<T>);
+  static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
   static_assert(FP % TK == 0, "tile must divide the plane");
   static_assert(THREADS % 32 == 0, "pencil CTA must be whole warps");
 };
@@ -45,8 +47,7 @@ struct PencilArgs {
   double* red;          // per-CTA spectral energy partial [rep][grid.x]
   int* nonfinite;       // set to 1 when a new coefficient is NaN/Inf
   const T* q;           // wavenumber table (N entries)
-  const cplx<T>* tw;
-  const cplx<T>* dtw;
+  const cplx<T>* tw;    // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
   int flags;
 };
@@ -56,26 +57,34 @@ struct PencilOps {
   using Cfg = PencilCfg<T, N, DCT>;
   static constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
 
+  // TK * N == THREADS * E: all E loads of a thread are issued before its stores
   static __device__ __forceinline__ void load_tile(cplx<T>* buf, const cplx<T>* __restrict__ src, int f0) {
-    for (int idx = threadIdx.x; idx < TK * N; idx += Cfg::THREADS) {
-      const int x = idx / TK, f = idx % TK;
-      buf[f * LS + pad(x)] = src[size_t(x) * FP + f0 + f];
+    cplx<T> tmp[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = threadIdx.x + Cfg::THREADS * e;
+      tmp[e] = src[size_t(idx / TK) * FP + f0 + idx % TK];
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = threadIdx.x + Cfg::THREADS * e;
+      buf[(idx % TK) * LS + pad(idx / TK)] = tmp[e];
     }
   }
   static __device__ __forceinline__ void store_tile(const cplx<T>* buf, cplx<T>* __restrict__ dst, int f0) {
-    for (int idx = threadIdx.x; idx < TK * N; idx += Cfg::THREADS) {
-      const int x = idx / TK, f = idx % TK;
-      dst[size_t(x) * FP + f0 + f] = buf[f * LS + pad(x)];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = threadIdx.x + Cfg::THREADS * e;
+      dst[size_t(idx / TK) * FP + f0 + idx % TK] = buf[(idx % TK) * LS + pad(idx / TK)];
     }
   }
 
   // forward x transform of the line; result in registers at kx = out_index<N,-1>
-  static __device__ __forceinline__ void forward(cplx<T> (&v)[E], cplx<T>* L, int t, const cplx<T>* __restrict__ tw,
-                                                 const cplx<T>* __restrict__ dtw) {
+  static __device__ __forceinline__ void forward(cplx<T> (&v)[E], cplx<T>* L, int t, const TwTables<T>& tw) {
     if constexpr (!DCT) {
-      fft_line<T, N, -1>(v, L, t, tw, [&](int i) { return L[pad(i)]; });
+      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(i)]; });
     } else {
-      fft_line<T, N, -1>(v, L, t, tw, [&](int i) { return L[pad(i < N / 2 ? 2 * i : 2 * (N - 1 - i) + 1)]; });
+      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(i < N / 2 ? 2 * i : 2 * (N - 1 - i) + 1)]; });
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
@@ -87,7 +96,7 @@ struct PencilOps {
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
-          cplx<T> w = __ldg(&dtw[k]);
+          cplx<T> w = tw.d[k];
           v[b * RL + r] = cadd<T>(cmul<T>(L[pad(k)], w), cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w)));
         }
     }
@@ -96,11 +105,10 @@ struct PencilOps {
   // inverse x transform of register values at kx = out_index<N,-1>; result
   // written to the line in natural x order (caller syncs before reading)
   static __device__ __forceinline__ void inverse_to_line(cplx<T> (&v)[E], cplx<T>* L, int t,
-                                                         const cplx<T>* __restrict__ tw,
-                                                         const cplx<T>* __restrict__ dtw) {
+                                                         const TwTables<T>& tw) {
     constexpr int RLI = radix_of<N, +1, Plan<N>::P - 1>();
     if constexpr (!DCT) {
-      fft_regs<T, N, +1>(v, L, t, tw);
+      fft_regs<T, N, +1>(v, L, t, tw.i);
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RLI; ++b)
@@ -113,14 +121,14 @@ struct PencilOps {
 #pragma unroll
         for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
       __syncwarp();
-      fft_line<T, N, +1>(v, L, t, tw, [&](int i) {
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
         cplx<T> a = L[pad(i)];
         cplx<T> u = a;
         if (i != 0) {
           cplx<T> bb = L[pad(N - i)];
           u = mk<T>(a.x + bb.y, a.y - bb.x);
         }
-        cplx<T> w = __ldg(&dtw[i]);
+        cplx<T> w = tw.d[i];
         w.y = -w.y;
         return cmul<T>(u, w);
       });
@@ -175,7 +183,9 @@ pencil_kernel(PencilArgs<T> a) {
   constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
-  double* scratch = reinterpret_cast<double*>(smem_raw + size_t(TK) * LS * sizeof(cplx<T>));
+  double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::RED_OFF);
+  const TwTables<T> tw =
+      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS);
 
   const int f0 = blockIdx.x * TK;
   const int rep = blockIdx.y;
@@ -209,15 +219,21 @@ pencil_kernel(PencilArgs<T> a) {
 
   if constexpr (MODE == kPencilStep) {
     Ops::load_tile(buf, a.src + plane_base, f0);
+    // the state W of this line, fetched while the transform runs
+    cplx<T> wreg[E];
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) wreg[b * RL + r] = wrow[out_index<N, -1>(t, b, r)];
     __syncthreads();
-    Ops::forward(v, L, t, a.tw, a.dtw);
+    Ops::forward(v, L, t, tw);
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
         const int kx = out_index<N, -1>(t, b, r);
         const T qx = __ldg(&a.q[kx]);
-        cplx<T> wv = wrow[kx];
+        cplx<T> wv = wreg[b * RL + r];
         const cplx<T> nh = v[b * RL + r];
         cplx<T> pn;
         if constexpr (!DCT) {
@@ -249,8 +265,10 @@ pencil_kernel(PencilArgs<T> a) {
     // gradient part of the energy of the current state from its partial P
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
-    Ops::forward(v, L, t, a.tw, a.dtw);
-    const double inv = 1.0 / a.pp.scale;
+    Ops::forward(v, L, t, tw);
+    // P = IDFT_x(scale psihat): its forward x transform is N scale psihat
+    // (REDFT10 after REDFT01: 2N scale psihat)
+    const double inv = 1.0 / (a.pp.scale * (DCT ? 2 * N : N));
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -273,12 +291,12 @@ pencil_kernel(PencilArgs<T> a) {
   } else {  // kPencilInit: W^0 from psi^0 and N(psi^0); P^0 from psi^0
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
-    Ops::forward(v, L, t, a.tw, a.dtw);
+    Ops::forward(v, L, t, tw);
     cplx<T> vn[E];
     __syncthreads();
     Ops::load_tile(buf, a.src2 + plane_base, f0);
     __syncthreads();
-    Ops::forward(vn, L, t, a.tw, a.dtw);
+    Ops::forward(vn, L, t, tw);
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -301,7 +319,7 @@ pencil_kernel(PencilArgs<T> a) {
   }
 
   if constexpr (MODE != kPencilEnergy) {
-    Ops::inverse_to_line(v, L, t, a.tw, a.dtw);
+    Ops::inverse_to_line(v, L, t, tw);
     __syncthreads();
     Ops::store_tile(buf, a.dst + plane_base, f0);
   }

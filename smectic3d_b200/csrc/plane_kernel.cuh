@@ -40,9 +40,10 @@ struct PlaneCfg {
   static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
   static constexpr int RL_INV = radix_of<N, +1, Plan<N>::P - 1>();
   static constexpr int RL_FWD = radix_of<N, -1, Plan<N>::P - 1>();
-  static constexpr size_t SMEM = size_t(LINES) * LS * sizeof(cplx<T>) + 64 * sizeof(double);
+  static constexpr size_t TW_OFF = size_t(LINES) * LS * sizeof(cplx<T>);
+  static constexpr size_t RED_OFF = TW_OFF + size_t(tw_total<N>()) * sizeof(cplx<T>);
+  static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
   static_assert(THREADS % 32 == 0, "plane CTA must be whole warps");
-  static_assert(THREADS >= N, "plane CTA must cover one column with one pass");
 };
 
 template <typename T>
@@ -54,27 +55,54 @@ struct PlaneArgs {
   double* psi_out;        // optional real psi out (dense)
   const double* psi_old;  // optional L1 reference (dense)
   double* red;            // per-CTA partial sums [rep][grid.x][3]
-  const cplx<T>* tw;      // w_N^m
-  const cplx<T>* dtw;     // exp(-i pi k / 2N)
+  const cplx<T>* tw;      // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
   int flags;
 };
 
-template <int CL>
+// Cluster barrier.  RELEASE orders this thread's earlier shared-memory writes
+// (local and remote) before the peers' reads; without it the barrier only
+// orders execution, which is what a write-after-read hand-over needs.
+template <int CL, bool RELEASE>
 __device__ __forceinline__ void cluster_sync() {
   if constexpr (CL == 1) {
     __syncthreads();
   } else {
-    cg::this_cluster().sync();
+    if constexpr (RELEASE) {
+      asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    } else {
+      asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
+    }
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
   }
 }
 
-template <int CL, typename P>
-__device__ __forceinline__ P* remote_ptr(P* local, int rank) {
+// Store into element ``off`` of the CTA-``rank`` copy of shared array ``buf``
+// (st.shared::cluster on the address mapa gives for that rank).
+__device__ __forceinline__ uint32_t dsmem_map(const void* p, int rank) {
+  const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
+  uint32_t r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_dsmem_raw(uint32_t a, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void st_dsmem_raw(uint32_t a, double2 v) {
+  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.x), "d"(v.y) : "memory");
+}
+__device__ __forceinline__ void st_dsmem_raw(uint32_t a, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_dsmem_raw(uint32_t a, double v) {
+  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
+}
+template <int CL, typename V>
+__device__ __forceinline__ void st_dsmem(V* buf, int rank, int off, V val) {
   if constexpr (CL == 1) {
-    return local;
+    buf[off] = val;
   } else {
-    return cg::this_cluster().map_shared_rank(local, rank);
+    st_dsmem_raw(dsmem_map(buf + off, rank), val);
   }
 }
 
@@ -84,14 +112,14 @@ __device__ __forceinline__ int mk_perm(int n) { return n < N / 2 ? 2 * n : 2 * (
 
 // first-pass input of REDFT01 (complex-linear): exp(+i pi i/2N) (X[i] - i X[N-i]), X[N] = 0
 template <typename T, int N>
-__device__ __forceinline__ cplx<T> dct3_pre(const cplx<T>* L, int i, const cplx<T>* __restrict__ dtw) {
+__device__ __forceinline__ cplx<T> dct3_pre(const cplx<T>* L, int i, const cplx<T>* dtw) {
   cplx<T> a = L[pad(i)];
   cplx<T> u = a;
   if (i != 0) {
     cplx<T> b = L[pad(N - i)];
     u = mk<T>(a.x + b.y, a.y - b.x);
   }
-  cplx<T> w = __ldg(&dtw[i]);
+  cplx<T> w = dtw[i];
   w.y = -w.y;
   return cmul<T>(u, w);
 }
@@ -126,13 +154,36 @@ struct PlaneOps {
   // ---- column phase, inverse direction ---------------------------------
   static __device__ void col_load(cplx<T>* buf, const cplx<T>* __restrict__ plane, int rank) {
     const int c0 = rank * NC;
-    for (int idx = threadIdx.x; idx < NC * N; idx += THREADS) {
-      const int ky = idx / NC, c = idx % NC;
-      buf[c * LS + pad(ky)] = plane[ky * (N / 2) + c0 + c];
+    // NC * N == THREADS * E: every thread issues its E loads before any store
+    cplx<T> tmp[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = threadIdx.x + THREADS * e;
+      tmp[e] = plane[(idx / NC) * (N / 2) + c0 + idx % NC];
+    }
+    constexpr int KPT = (N + THREADS - 1) / THREADS;  // ky per thread for the kz=0 / N/2 columns
+    cplx<T> nyq[KPT];
+    if constexpr (!DCT) {
+      if (rank == 0) {
+#pragma unroll
+        for (int m = 0; m < KPT; ++m) {
+          const int ky = threadIdx.x + m * THREADS;
+          if (ky < N) nyq[m] = plane[N * (N / 2) + ky];
+        }
+      }
+    }
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = threadIdx.x + THREADS * e;
+      buf[(idx % NC) * LS + pad(idx / NC)] = tmp[e];
     }
     if constexpr (!DCT) {
       if (rank == 0) {
-        for (int ky = threadIdx.x; ky < N; ky += THREADS) buf[NC * LS + pad(ky)] = plane[N * (N / 2) + ky];
+#pragma unroll
+        for (int m = 0; m < KPT; ++m) {
+          const int ky = threadIdx.x + m * THREADS;
+          if (ky < N) buf[NC * LS + pad(ky)] = nyq[m];
+        }
       }
     }
     __syncthreads();
@@ -140,35 +191,41 @@ struct PlaneOps {
       if (rank == 0) {
         // Hermitian projection in ky of the kz=0 and kz=N/2 columns (the real
         // part FFTW's c2r keeps on those planes), packed as F0 + i FN.
-        const int ky = threadIdx.x;  // THREADS >= N
-        cplx<T> out = mk<T>(T(0), T(0));
-        if (ky < N) {
-          const int km = (N - ky) & (N - 1);
-          cplx<T> a0 = buf[pad(ky)], a1 = buf[pad(km)];
-          cplx<T> b0 = buf[NC * LS + pad(ky)], b1 = buf[NC * LS + pad(km)];
-          const T f0x = T(0.5) * (a0.x + a1.x), f0y = T(0.5) * (a0.y - a1.y);
-          const T fnx = T(0.5) * (b0.x + b1.x), fny = T(0.5) * (b0.y - b1.y);
-          out = mk<T>(f0x - fny, f0y + fnx);
+        cplx<T> out[KPT];
+#pragma unroll
+        for (int m = 0; m < KPT; ++m) {
+          const int ky = threadIdx.x + m * THREADS;
+          if (ky < N) {
+            const int km = (N - ky) & (N - 1);
+            cplx<T> a0 = buf[pad(ky)], a1 = buf[pad(km)];
+            cplx<T> b0 = buf[NC * LS + pad(ky)], b1 = buf[NC * LS + pad(km)];
+            const T f0x = T(0.5) * (a0.x + a1.x), f0y = T(0.5) * (a0.y - a1.y);
+            const T fnx = T(0.5) * (b0.x + b1.x), fny = T(0.5) * (b0.y - b1.y);
+            out[m] = mk<T>(f0x - fny, f0y + fnx);
+          }
         }
         __syncthreads();
-        if (ky < N) buf[pad(ky)] = out;
+#pragma unroll
+        for (int m = 0; m < KPT; ++m) {
+          const int ky = threadIdx.x + m * THREADS;
+          if (ky < N) buf[pad(ky)] = out[m];
+        }
         __syncthreads();
       }
     }
   }
 
   // inverse y transform of the owned columns, then scatter into row layout
-  static __device__ void col_inverse_to_rows(cplx<T>* buf, int rank, const cplx<T>* __restrict__ tw,
-                                             const cplx<T>* __restrict__ dtw) {
+  static __device__ void col_inverse_to_rows(cplx<T>* buf, int rank, const TwTables<T>& tw) {
     const int line = threadIdx.x / G, t = threadIdx.x % G;
     cplx<T>* L = buf + line * LS;
     cplx<T> v[E];
     if constexpr (!DCT) {
-      fft_line<T, N, +1>(v, L, t, tw, [&](int i) { return L[pad(i)]; });
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return L[pad(i)]; });
     } else {
-      fft_line<T, N, +1>(v, L, t, tw, [&](int i) { return dct3_pre<T, N>(L, i, dtw); });
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return dct3_pre<T, N>(L, i, tw.d); });
     }
-    cluster_sync<CL>();
+    cluster_sync<CL, false>();
     const int kc = rank * NC + line;  // global complex column
     constexpr int RL = Cfg::RL_INV;
 #pragma unroll
@@ -179,29 +236,27 @@ struct PlaneOps {
         const cplx<T> val = v[b * RL + r];
         if constexpr (!DCT) {
           const int dest = n / ROWS, yl = n % ROWS;
-          cplx<T>* rb = remote_ptr<CL>(buf, dest);
-          rb[(yl >> 1) * LS + pad((yl & 1) * (N / 2) + kc)] = val;
+          st_dsmem<CL>(buf, dest, (yl >> 1) * LS + pad((yl & 1) * (N / 2) + kc), val);
         } else {
           const int y = mk_perm<N>(n);
           const int dest = y / ROWS, yl = y % ROWS;
-          T* rb = reinterpret_cast<T*>(remote_ptr<CL>(buf, dest));
+          T* rb = reinterpret_cast<T*>(buf);
           const int base = (yl >> 1) * LS;
-          rb[2 * (base + pad(2 * kc)) + (yl & 1)] = val.x;
-          rb[2 * (base + pad(2 * kc + 1)) + (yl & 1)] = val.y;
+          st_dsmem<CL>(rb, dest, 2 * (base + pad(2 * kc)) + (yl & 1), val.x);
+          st_dsmem<CL>(rb, dest, 2 * (base + pad(2 * kc + 1)) + (yl & 1), val.y);
         }
       }
-    cluster_sync<CL>();
+    cluster_sync<CL, true>();
   }
 
   // ---- row phase -------------------------------------------------------
   // inverse z transform of row pair ``line``; v slot holds psi(y0, z), psi(y0+1, z)
   static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], cplx<T>* L, int t,
-                                                     const cplx<T>* __restrict__ tw,
-                                                     const cplx<T>* __restrict__ dtw) {
+                                                     const TwTables<T>& tw) {
     if constexpr (!DCT) {
-      fft_line<T, N, +1>(v, L, t, tw, [&](int i) { return c2r_pre<T, N>(L, i); });
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return c2r_pre<T, N>(L, i); });
     } else {
-      fft_line<T, N, +1>(v, L, t, tw, [&](int i) { return dct3_pre<T, N>(L, i, dtw); });
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return dct3_pre<T, N>(L, i, tw.d); });
     }
   }
 
@@ -215,8 +270,8 @@ struct PlaneOps {
 
   // forward z transform from registers, then scatter to column layout
   static __device__ void row_forward_to_cols(cplx<T> (&v)[E], cplx<T>* buf, cplx<T>* L, int rank, int line, int t,
-                                             const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ dtw) {
-    fft_regs<T, N, -1>(v, L, t, tw);
+                                             const TwTables<T>& tw) {
+    fft_regs<T, N, -1>(v, L, t, tw.f);
     constexpr int RL = Cfg::RL_FWD;
     __syncwarp();
 #pragma unroll
@@ -244,17 +299,16 @@ struct PlaneOps {
             ob[s] = mk<T>(T(0.5) * (zk.y + zm.y), T(0.5) * (zm.x - zk.x));
           }
         }
-      cluster_sync<CL>();
+      cluster_sync<CL, false>();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
         for (int r = 0; r < RL / 2; ++r) {
           const int k = out_index<N, -1>(t, b, r);
           const int s = b * (RL / 2) + r;
-          cplx<T>* cb = remote_ptr<CL>(buf, k / NC);
-          cplx<T>* col = cb + (k % NC) * LS;
-          col[pad(y0)] = oa[s];
-          col[pad(y0 + 1)] = ob[s];
+          const int col = (k % NC) * LS;
+          st_dsmem<CL>(buf, k / NC, col + pad(y0), oa[s]);
+          st_dsmem<CL>(buf, k / NC, col + pad(y0 + 1), ob[s]);
         }
     } else {
       cplx<T> o[E];
@@ -263,35 +317,36 @@ struct PlaneOps {
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
-          cplx<T> w = __ldg(&dtw[k]);
+          cplx<T> w = tw.d[k];
           cplx<T> a = cmul<T>(L[pad(k)], w);
           cplx<T> bm = cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w));
           o[b * RL + r] = cadd<T>(a, bm);
         }
-      cluster_sync<CL>();
+      cluster_sync<CL, false>();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
           const int p = k >> 1;
-          T* cb = reinterpret_cast<T*>(remote_ptr<CL>(buf, p / NC) + (p % NC) * LS);
-          cb[2 * pad(y0) + (k & 1)] = o[b * RL + r].x;
-          cb[2 * pad(y0 + 1) + (k & 1)] = o[b * RL + r].y;
+          T* rb = reinterpret_cast<T*>(buf);
+          const int col = 2 * (p % NC) * LS;
+          st_dsmem<CL>(rb, p / NC, col + 2 * pad(y0) + (k & 1), o[b * RL + r].x);
+          st_dsmem<CL>(rb, p / NC, col + 2 * pad(y0 + 1) + (k & 1), o[b * RL + r].y);
         }
     }
-    cluster_sync<CL>();
+    cluster_sync<CL, true>();
   }
 
   // ---- column phase, forward direction ---------------------------------
   static __device__ void col_forward_store(cplx<T>* buf, cplx<T>* __restrict__ plane, int rank,
-                                           const cplx<T>* __restrict__ tw, const cplx<T>* __restrict__ dtw) {
+                                           const TwTables<T>& tw) {
     const int line = threadIdx.x / G, t = threadIdx.x % G;
     cplx<T>* L = buf + line * LS;
     cplx<T> v[E];
     constexpr int RL = Cfg::RL_FWD;
     if constexpr (!DCT) {
-      fft_line<T, N, -1>(v, L, t, tw, [&](int i) { return L[pad(i)]; });
+      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(i)]; });
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
@@ -300,22 +355,30 @@ struct PlaneOps {
       __syncthreads();
       if (rank == 0) {
         // unpack F0 + i FN of the kz=0 / kz=N/2 columns
-        const int ky = threadIdx.x;
-        cplx<T> f0 = mk<T>(T(0), T(0)), fn = f0;
-        if (ky < N) {
-          cplx<T> z = buf[pad(ky)], zm = buf[pad((N - ky) & (N - 1))];
-          f0 = mk<T>(T(0.5) * (z.x + zm.x), T(0.5) * (z.y - zm.y));
-          fn = mk<T>(T(0.5) * (z.y + zm.y), T(0.5) * (zm.x - z.x));
+        constexpr int KPT = (N + THREADS - 1) / THREADS;
+        cplx<T> f0[KPT], fn[KPT];
+#pragma unroll
+        for (int m = 0; m < KPT; ++m) {
+          const int ky = threadIdx.x + m * THREADS;
+          if (ky < N) {
+            cplx<T> z = buf[pad(ky)], zm = buf[pad((N - ky) & (N - 1))];
+            f0[m] = mk<T>(T(0.5) * (z.x + zm.x), T(0.5) * (z.y - zm.y));
+            fn[m] = mk<T>(T(0.5) * (z.y + zm.y), T(0.5) * (zm.x - z.x));
+          }
         }
         __syncthreads();
-        if (ky < N) {
-          buf[pad(ky)] = f0;
-          buf[NC * LS + pad(ky)] = fn;
+#pragma unroll
+        for (int m = 0; m < KPT; ++m) {
+          const int ky = threadIdx.x + m * THREADS;
+          if (ky < N) {
+            buf[pad(ky)] = f0[m];
+            buf[NC * LS + pad(ky)] = fn[m];
+          }
         }
         __syncthreads();
       }
     } else {
-      fft_line<T, N, -1>(v, L, t, tw, [&](int i) { return L[pad(mk_perm<N>(i))]; });
+      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(mk_perm<N>(i))]; });
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
@@ -327,7 +390,7 @@ struct PlaneOps {
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
-          cplx<T> w = __ldg(&dtw[k]);
+          cplx<T> w = tw.d[k];
           v[b * RL + r] = cadd<T>(cmul<T>(L[pad(k)], w), cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w)));
         }
       __syncwarp();
@@ -338,9 +401,10 @@ struct PlaneOps {
       __syncthreads();
     }
     const int c0 = rank * NC;
-    for (int idx = threadIdx.x; idx < NC * N; idx += THREADS) {
-      const int ky = idx / NC, c = idx % NC;
-      plane[ky * (N / 2) + c0 + c] = buf[c * LS + pad(ky)];
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int idx = threadIdx.x + THREADS * e;
+      plane[(idx / NC) * (N / 2) + c0 + idx % NC] = buf[(idx % NC) * LS + pad(idx / NC)];
     }
     if constexpr (!DCT) {
       if (rank == 0) {
@@ -393,7 +457,9 @@ plane_kernel(PlaneArgs<T> a) {
   constexpr int RL = Cfg::RL_INV;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
-  double* scratch = reinterpret_cast<double*>(smem_raw + size_t(Cfg::LINES) * LS * sizeof(cplx<T>));
+  double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::RED_OFF);
+  const TwTables<T> tw =
+      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS);
 
   int rank = 0;
   if constexpr (CL > 1) rank = int(cg::this_cluster().block_rank());
@@ -408,8 +474,8 @@ plane_kernel(PlaneArgs<T> a) {
 
   if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi) {
     Ops::col_load(buf, a.src + plane_off, rank);
-    Ops::col_inverse_to_rows(buf, rank, a.tw, a.dtw);
-    Ops::row_inverse(v, L, t, a.tw, a.dtw);
+    Ops::col_inverse_to_rows(buf, rank, tw);
+    Ops::row_inverse(v, L, t, tw);
 
     if (a.flags & (kFlPsiOut | kFlL1 | kFlEnergy)) {
       KahanSum s0, s1, s2;
@@ -448,8 +514,8 @@ plane_kernel(PlaneArgs<T> a) {
     }
     if constexpr (MODE == kPlaneStep) {
       row_nonlin<T, N, CL, DCT>(v, L, t, a.pp);
-      Ops::row_forward_to_cols(v, buf, L, rank, line, t, a.tw, a.dtw);
-      Ops::col_forward_store(buf, a.dst + plane_off, rank, a.tw, a.dtw);
+      Ops::row_forward_to_cols(v, buf, L, rank, line, t, tw);
+      Ops::col_forward_store(buf, a.dst + plane_off, rank, tw);
     }
   } else {  // kPlaneInit: real psi -> partial spectra of psi (dst2) and N(psi) (dst)
     const double* src = a.psi_in + real_off;
@@ -477,8 +543,8 @@ plane_kernel(PlaneArgs<T> a) {
           }
           v[b * R0 + r] = mk<T>(pa, pb);
         }
-      Ops::row_forward_to_cols(v, buf, L, rank, line, t, a.tw, a.dtw);
-      Ops::col_forward_store(buf, (field == 0 ? a.dst2 : a.dst) + plane_off, rank, a.tw, a.dtw);
+      Ops::row_forward_to_cols(v, buf, L, rank, line, t, tw);
+      Ops::col_forward_store(buf, (field == 0 ? a.dst2 : a.dst) + plane_off, rank, tw);
     }
   }
 }

@@ -132,14 +132,15 @@ int sh_create(const sh_params* p, sh_handle** out) {
     return fail(nullptr, SH_EINVAL, "advection is defined for the periodic boundary only");
   if (p->advection) return fail(nullptr, SH_EUNSUPPORTED, "advection is not built into this library version");
   if (p->sub_sigma != 0.0) return fail(nullptr, SH_EUNSUPPORTED, "substrate penalty is not built into this library version");
+  if (p->variant < 0) return fail(nullptr, SH_EINVAL, "variant must be >= 0");
 
   SolverBase* s = nullptr;
   const bool f32 = p->precision == SH_FP32;
   if (p->boundary == SH_PERIODIC)
-    s = f32 ? make_solver_f32_periodic(p->n) : make_solver_f64_periodic(p->n);
+    s = f32 ? make_solver_f32_periodic(p->n, p->variant) : make_solver_f64_periodic(p->n, p->variant);
   else
-    s = f32 ? make_solver_f32_neumann(p->n) : make_solver_f64_neumann(p->n);
-  if (!s) return fail(nullptr, SH_EUNSUPPORTED, "size not built");
+    s = f32 ? make_solver_f32_neumann(p->n, p->variant) : make_solver_f64_neumann(p->n, p->variant);
+  if (!s) return fail(nullptr, SH_EUNSUPPORTED, "this size / variant is not built");
   std::unique_ptr<sh_handle> h(new sh_handle);
   h->s = s;
   s->p = *p;
@@ -364,6 +365,23 @@ int sh_host_alloc(size_t bytes, void** out) {
 int sh_host_free(void* p) {
   cudaError_t e = cudaFreeHost(p);
   return e == cudaSuccess ? SH_OK : SH_ECUDA;
+}
+
+int sh_profile_steps(sh_handle* h, int nsteps, double* ms_pencil, double* ms_plane) {
+  if (!h || !h->s || !ms_pencil || !ms_plane) return fail(h, SH_EINVAL, "null argument");
+  SolverBase* s = h->s;
+  if (!s->ready) return fail(h, SH_ESTATE, "psi was never set");
+  for (auto& e : s->prof_ev)
+    if (!e) API_CUDA(h, cudaEventCreate(&e));
+  double ms[2] = {0.0, 0.0};
+  s->prof_ms = ms;
+  int rc = s->step_async(nsteps);
+  s->prof_ms = nullptr;
+  if (rc) return rc;
+  API_CUDA(h, cudaStreamSynchronize(s->stream));
+  *ms_pencil = ms[0];
+  *ms_plane = ms[1];
+  return SH_OK;
 }
 
 int sh_synchronize(sh_handle* h) {

@@ -46,6 +46,7 @@ struct SolverBase {
   std::vector<double> l1_last;
   int l1_count = 0;
   bool ready = false;
+  bool psi0_valid = false;  // d_psi holds psi^0 exactly as uploaded
 
   virtual ~SolverBase() {
     if (stream) cudaStreamSynchronize(stream);
@@ -57,12 +58,17 @@ struct SolverBase {
     cudaFree(d_red_spec);
     cudaFree(d_scalar);
     cudaFree(d_trace);
+    for (auto& e : prof_ev)
+      if (e) cudaEventDestroy(e);
     if (stream) cudaStreamDestroy(stream);
   }
   size_t n3() const { return size_t(p.n) * p.n * p.n; }
   virtual int setup() = 0;
   virtual int init_from_psi() = 0;     // d_psi holds psi^0
   virtual int step_async(int n) = 0;
+  // per-launch event timing of the two passes (nullptr: off)
+  double* prof_ms = nullptr;
+  cudaEvent_t prof_ev[3] = {nullptr, nullptr, nullptr};
   virtual int psi_to_dpsi() = 0;       // current psi -> d_psi
   virtual int energy_now(double* host) = 0;
   virtual size_t state_bytes() const = 0;
@@ -79,8 +85,7 @@ struct Solver final : SolverBase {
   cplx<T>* W = nullptr;
   cplx<T>* P = nullptr;
   cplx<T>* Nt = nullptr;
-  cplx<T>* tw = nullptr;
-  cplx<T>* dtw = nullptr;
+  cplx<T>* tw = nullptr;  // [forward | inverse | quarter-wave] twiddle table
   T* q = nullptr;
 
   ~Solver() override {
@@ -89,7 +94,6 @@ struct Solver final : SolverBase {
     cudaFree(P);
     cudaFree(Nt);
     cudaFree(tw);
-    cudaFree(dtw);
     cudaFree(q);
   }
 
@@ -129,23 +133,13 @@ struct Solver final : SolverBase {
     SHB_CUDA(cudaMalloc(&W, fe * sizeof(cplx<T>)));
     SHB_CUDA(cudaMalloc(&P, fe * sizeof(cplx<T>)));
     SHB_CUDA(cudaMalloc(&Nt, fe * sizeof(cplx<T>)));
-    SHB_CUDA(cudaMalloc(&tw, N * sizeof(cplx<T>)));
-    SHB_CUDA(cudaMalloc(&dtw, N * sizeof(cplx<T>)));
+    SHB_CUDA(cudaMalloc(&tw, tw_total<N>() * sizeof(cplx<T>)));
     SHB_CUDA(cudaMalloc(&q, N * sizeof(T)));
     SHB_CUDA(cudaMalloc(&d_red_plane, size_t(p.batch) * N * CL * 3 * sizeof(double)));
     SHB_CUDA(cudaMalloc(&d_red_spec, size_t(p.batch) * QC::TILES * sizeof(double)));
-    // twiddles w_N^m = exp(-2 pi i m / N), quarter-wave exp(-i pi k / 2N), wavenumbers
-    std::vector<cplx<T>> htw(N), hdtw(N);
+    std::vector<cplx<T>> htw;
+    host_twiddles<T, N>(htw);
     std::vector<T> hq(N);
-    const long double pi = 3.141592653589793238462643383279502884L;
-    for (int m = 0; m < N; ++m) {
-      long double a = -2.0L * pi * m / N;
-      htw[m].x = T(std::cos(a));
-      htw[m].y = T(std::sin(a));
-      long double b = -pi * m / (2.0L * N);
-      hdtw[m].x = T(std::cos(b));
-      hdtw[m].y = T(std::sin(b));
-    }
     if (!DCT) {
       // periodicFFT/pf3d.cpp:166-190 (Nyquist entry +pi/dx)
       for (int i = 0; i < N; ++i)
@@ -154,8 +148,7 @@ struct Solver final : SolverBase {
       // cosFFT/mesabi/cosNoAdvMorph.cpp:216-231
       for (int i = 0; i < N; ++i) hq[i] = T(M_PI * i / (p.dx * N));
     }
-    SHB_CUDA(cudaMemcpy(tw, htw.data(), N * sizeof(cplx<T>), cudaMemcpyHostToDevice));
-    SHB_CUDA(cudaMemcpy(dtw, hdtw.data(), N * sizeof(cplx<T>), cudaMemcpyHostToDevice));
+    SHB_CUDA(cudaMemcpy(tw, htw.data(), htw.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice));
     SHB_CUDA(cudaMemcpy(q, hq.data(), N * sizeof(T), cudaMemcpyHostToDevice));
     int rc;
     if ((rc = set_attrs(plane_fn<kPlaneStep>(), PC::SMEM, true))) return rc;
@@ -197,7 +190,6 @@ struct Solver final : SolverBase {
   PlaneArgs<T> plane_args() const {
     PlaneArgs<T> a{};
     a.tw = tw;
-    a.dtw = dtw;
     a.pp = point_params();
     a.red = d_red_plane;
     return a;
@@ -205,7 +197,6 @@ struct Solver final : SolverBase {
   PencilArgs<T> pencil_args() const {
     PencilArgs<T> a{};
     a.tw = tw;
-    a.dtw = dtw;
     a.q = q;
     a.pp = point_params();
     a.red = d_red_spec;
@@ -240,6 +231,7 @@ struct Solver final : SolverBase {
       SHB_CUDA(cudaMemcpyAsync(d_stash, d_psi, size_t(p.batch) * n3() * sizeof(double), cudaMemcpyDeviceToDevice,
                                stream));
     steps = 0;
+    psi0_valid = true;
     l1_count = 0;
     energy_trace.clear();
     ready = true;
@@ -265,7 +257,9 @@ struct Solver final : SolverBase {
       b.w = W;
       b.dst = P;
       b.flags = trace ? kFlEnergy : 0;
+      if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[0], stream));
       if ((rc = launch_pencil<kPencilStep>(b))) return rc;
+      if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
       PlaneArgs<T> a = plane_args();
       a.src = P;
       a.dst = Nt;
@@ -273,6 +267,15 @@ struct Solver final : SolverBase {
       a.psi_old = d_stash;
       a.psi_out = d_stash;
       if ((rc = launch_plane<kPlaneStep>(a))) return rc;
+      if (prof_ms) {
+        float t0, t1;
+        SHB_CUDA(cudaEventRecord(prof_ev[2], stream));
+        SHB_CUDA(cudaEventSynchronize(prof_ev[2]));
+        SHB_CUDA(cudaEventElapsedTime(&t0, prof_ev[0], prof_ev[1]));
+        SHB_CUDA(cudaEventElapsedTime(&t1, prof_ev[1], prof_ev[2]));
+        prof_ms[0] += t0;
+        prof_ms[1] += t1;
+      }
       if (trace && (rc = finalize(0, d_trace + size_t(s) * p.batch))) return rc;
       if (l1_now) {
         if ((rc = finalize(1, d_scalar))) return rc;
@@ -283,19 +286,23 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
-  int psi_to_dpsi() override { return plane_getpsi(false); }
+  int psi_to_dpsi() override {
+    if (steps == 0 && psi0_valid) return SH_OK;  // d_psi still holds the uploaded psi^0
+    psi0_valid = false;
+    return plane_getpsi(true, false);
+  }
 
-  int plane_getpsi(bool energy) {
+  int plane_getpsi(bool write_psi, bool energy) {
     PlaneArgs<T> a = plane_args();
     a.src = P;
     a.psi_out = d_psi;
-    a.flags = kFlPsiOut | (energy ? kFlEnergy : 0);
+    a.flags = (write_psi ? kFlPsiOut : 0) | (energy ? kFlEnergy : 0);
     return launch_plane<kPlaneGetPsi>(a);
   }
 
   int energy_now(double* host) override {
     int rc;
-    if ((rc = plane_getpsi(true))) return rc;
+    if ((rc = plane_getpsi(false, true))) return rc;
     PencilArgs<T> b = pencil_args();
     b.src = P;
     b.flags = kFlEnergy;
@@ -324,14 +331,15 @@ struct Solver final : SolverBase {
     SHB_CUDA(cudaMemcpyAsync(Nt, h + 2 * fb, fb, cudaMemcpyHostToDevice, stream));
     SHB_CUDA(cudaStreamSynchronize(stream));
     ready = true;
+    psi0_valid = false;
     return SH_OK;
   }
 };
 
 // factory: defined per precision / boundary in the instantiation units
-SolverBase* make_solver_f32_periodic(int n);
-SolverBase* make_solver_f64_periodic(int n);
-SolverBase* make_solver_f32_neumann(int n);
-SolverBase* make_solver_f64_neumann(int n);
+SolverBase* make_solver_f32_periodic(int n, int variant);
+SolverBase* make_solver_f64_periodic(int n, int variant);
+SolverBase* make_solver_f32_neumann(int n, int variant);
+SolverBase* make_solver_f64_neumann(int n, int variant);
 
 }  // namespace shb

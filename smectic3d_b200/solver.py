@@ -41,6 +41,7 @@ class Params:
     sub_sigma: float = 0.0
     sub_z0: float = 1e-4
     eps_per_replica: tuple | None = None
+    variant: int = 0                 # plane-pass cluster size override (0 = default)
 
     @staticmethod
     def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":
@@ -57,6 +58,7 @@ class Params:
         p.precision = {"fp64": L.SH_FP64, "fp32": L.SH_FP32}[self.precision]
         p.l1_interval = self.l1_interval
         p.energy_trace = int(bool(self.energy_trace))
+        p.variant = int(self.variant)
         for k in ("dx", "dt", "eps", "beta", "gamma", "alpha", "q0", "eta", "rho", "w_mid", "sub_sigma", "sub_z0"):
             setattr(p, k, float(getattr(self, k)))
         keep = None
@@ -132,6 +134,12 @@ class Solver:
             out = np.empty(self.shape, dtype=np.float64)
         self._chk(self.lib.sh_run(self.h, a.ctypes.data, int(nsteps), out.ctypes.data, L.SH_LAYOUT_DENSE))
         return out
+
+    def profile_steps(self, nsteps: int):
+        """Per-pass device time (ms) of ``nsteps`` steps: (pencil, plane)."""
+        a, b = C.c_double(), C.c_double()
+        self._chk(self.lib.sh_profile_steps(self.h, int(nsteps), C.byref(a), C.byref(b)))
+        return a.value, b.value
 
     def synchronize(self):
         self._chk(self.lib.sh_synchronize(self.h))
