@@ -162,18 +162,9 @@ __device__ __forceinline__ Mult<T> make_mult(T qx, T qy, T qz, T eps, const Poin
   return m;
 }
 
-// CNAB2 (or IMEX Euler) update of one real spectral coefficient pair
-template <typename T>
-__device__ __forceinline__ T update_one(T& w, T nh, const Mult<T>& m, const PointParams& pp) {
-  if (pp.scheme == kCNAB2) {
-    const T psi_new = (w + T(1.5 * pp.dt) * nh) / m.c2;
-    w = m.c1 * psi_new - T(0.5 * pp.dt) * nh;
-    return psi_new;
-  }
-  const T psi_new = (w + T(pp.dt) * nh) / (T(1) - T(pp.dt) * m.a_lin);
-  w = psi_new;
-  return psi_new;
-}
+// correctly rounded reciprocal
+__device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 
 template <typename T, int N, bool DCT, int MODE>
 __global__ void __launch_bounds__(PencilCfg<T, N, DCT>::THREADS)
@@ -227,40 +218,69 @@ pencil_kernel(PencilArgs<T> a) {
       for (int r = 0; r < RL; ++r) wreg[b * RL + r] = wrow[out_index<N, -1>(t, b, r)];
     __syncthreads();
     Ops::forward(v, L, t, tw);
+    // mode-independent constants of the update; the (ky, kz) part of |q|^2 is
+    // fixed for the line
+    const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha);
+    const T h = T(0.5 * a.pp.dt), h3 = T(1.5 * a.pp.dt), dtT = T(a.pp.dt);
+    const T qyz0 = qy * qy + qz0 * qz0 - q02;
+    const T qyz1 = qy * qy + qz1 * qz1 - q02;
+    const bool cnab2 = a.pp.scheme == kCNAB2;
+    bool bad = false;
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
         const int kx = out_index<N, -1>(t, b, r);
         const T qx = __ldg(&a.q[kx]);
+        const T qx2 = qx * qx;
         cplx<T> wv = wreg[b * RL + r];
         const cplx<T> nh = v[b * RL + r];
         cplx<T> pn;
-        if constexpr (!DCT) {
-          const Mult<T> m = make_mult<T>(qx, qy, qz0, eps, a.pp);
-          pn.x = update_one<T>(wv.x, nh.x, m, a.pp);
-          pn.y = update_one<T>(wv.y, nh.y, m, a.pp);
-          if (want_energy) {
-            const double d = double(a.pp.q0) * a.pp.q0 - double(m.mq2);
-            const double wgt = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
-            acc.add(wgt * d * d * (double(pn.x) * pn.x + double(pn.y) * pn.y));
+        // psihat^{n+1} = (W + 3dt/2 Nhat) / C2,  W' = C1 psihat^{n+1} - dt/2 Nhat  (CNAB2)
+        // psihat^{n+1} = (psihat + dt Nhat) / (1 - dt aLin),  W' = psihat^{n+1} (IMEX Euler)
+        const T d0 = qx2 + qyz0;
+        const T a0 = eps - alpha * d0 * d0;
+        if (cnab2) {
+          const T inv0 = rcp_rn(T(1) - h * a0), c10 = T(1) + h * a0;
+          pn.x = (wv.x + h3 * nh.x) * inv0;
+          wv.x = c10 * pn.x - h * nh.x;
+          if constexpr (!DCT) {
+            pn.y = (wv.y + h3 * nh.y) * inv0;
+            wv.y = c10 * pn.y - h * nh.y;
+          } else {
+            const T d1 = qx2 + qyz1;
+            const T a1 = eps - alpha * d1 * d1;
+            const T inv1 = rcp_rn(T(1) - h * a1);
+            pn.y = (wv.y + h3 * nh.y) * inv1;
+            wv.y = (T(1) + h * a1) * pn.y - h * nh.y;
           }
         } else {
-          const Mult<T> m0 = make_mult<T>(qx, qy, qz0, eps, a.pp);
-          const Mult<T> m1 = make_mult<T>(qx, qy, qz1, eps, a.pp);
-          pn.x = update_one<T>(wv.x, nh.x, m0, a.pp);
-          pn.y = update_one<T>(wv.y, nh.y, m1, a.pp);
-          if (want_energy) {
+          const T inv0 = rcp_rn(T(1) - dtT * a0);
+          pn.x = (wv.x + dtT * nh.x) * inv0;
+          if constexpr (!DCT) {
+            pn.y = (wv.y + dtT * nh.y) * inv0;
+          } else {
+            const T d1 = qx2 + qyz1;
+            pn.y = (wv.y + dtT * nh.y) * rcp_rn(T(1) - dtT * (eps - alpha * d1 * d1));
+          }
+          wv = pn;
+        }
+        if (want_energy) {
+          if constexpr (!DCT) {
+            const double d = double(d0);
+            const double wgt = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
+            acc.add(wgt * d * d * (double(pn.x) * pn.x + double(pn.y) * pn.y));
+          } else {
             const double wxy = (kx == 0 ? 0.5 : 1.0) * (ky == 0 ? 0.5 : 1.0);
-            const double d0 = double(a.pp.q0) * a.pp.q0 - double(m0.mq2);
-            const double d1 = double(a.pp.q0) * a.pp.q0 - double(m1.mq2);
-            acc.add(wxy * ((kz == 0 ? 0.5 : 1.0) * d0 * d0 * double(pn.x) * pn.x + d1 * d1 * double(pn.y) * pn.y));
+            const double e0 = double(d0), e1 = double(qx2 + qyz1);
+            acc.add(wxy * ((kz == 0 ? 0.5 : 1.0) * e0 * e0 * double(pn.x) * pn.x + e1 * e1 * double(pn.y) * pn.y));
           }
         }
-        if (!isfinite(pn.x) || !isfinite(pn.y)) *a.nonfinite = 1;
+        bad |= !isfinite(pn.x) || !isfinite(pn.y);
         wrow[kx] = wv;
         v[b * RL + r] = cscale<T>(pn, scale);
       }
+    if (bad) *a.nonfinite = 1;
   } else if constexpr (MODE == kPencilEnergy) {
     // gradient part of the energy of the current state from its partial P
     Ops::load_tile(buf, a.src + plane_base, f0);

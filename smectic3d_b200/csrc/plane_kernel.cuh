@@ -28,6 +28,8 @@ namespace shb {
 
 enum PlaneMode : int { kPlaneStep = 0, kPlaneInit = 1, kPlaneGetPsi = 2 };
 
+__host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
 template <typename T, int N, int CL, bool DCT>
 struct PlaneCfg {
   static constexpr int E = Plan<N>::E;
@@ -40,9 +42,26 @@ struct PlaneCfg {
   static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
   static constexpr int RL_INV = radix_of<N, +1, Plan<N>::P - 1>();
   static constexpr int RL_FWD = radix_of<N, -1, Plan<N>::P - 1>();
-  static constexpr size_t TW_OFF = size_t(LINES) * LS * sizeof(cplx<T>);
-  static constexpr size_t RED_OFF = TW_OFF + size_t(tw_total<N>()) * sizeof(cplx<T>);
+  // Exchange blocks between the CTAs of a cluster (CL > 1), one per
+  // (source, destination) pair, padded rows so that both the writer and the
+  // reader access shared memory without bank conflicts:
+  //   column -> row, periodic : [row yl][column c]        stride NC + 1
+  //   column -> row, Neumann  : [row pair q][kz local]    stride 2 NC + 1
+  //   row -> column (both)    : [row yl][column c]        stride NC + 1
+  static constexpr int SA = DCT ? 2 * NC + 1 : NC + 1;
+  static constexpr int SBs = NC + 1;
+  static constexpr int BLK_A = DCT ? (ROWS / 2) * (2 * NC + 1) : ROWS * (NC + 1);
+  static constexpr int BLK_B = ROWS * (NC + 1);
+  static constexpr int BLK = ((BLK_A > BLK_B ? BLK_A : BLK_B) + 1) / 2 * 2;  // even: 16-byte blocks
+  static constexpr size_t LB_BYTES = align_up(size_t(LINES) * LS * sizeof(cplx<T>), 128);
+  static constexpr size_t XB_BYTES = CL > 1 ? align_up(size_t(CL) * BLK * sizeof(cplx<T>), 128) : 0;
+  static constexpr size_t SB_OFF = LB_BYTES;
+  static constexpr size_t RB_OFF = SB_OFF + XB_BYTES;
+  static constexpr size_t TW_OFF = RB_OFF + XB_BYTES;
+  static constexpr size_t MB_OFF = align_up(TW_OFF + size_t(tw_total<N>()) * sizeof(cplx<T>), 16);
+  static constexpr size_t RED_OFF = MB_OFF + 16;
   static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
+  static constexpr bool fits = SMEM <= 227 * 1024;  // per-CTA shared memory limit of sm_100
   static_assert(THREADS % 32 == 0, "plane CTA must be whole warps");
 };
 
@@ -55,6 +74,7 @@ struct PlaneArgs {
   double* psi_out;        // optional real psi out (dense)
   const double* psi_old;  // optional L1 reference (dense)
   double* red;            // per-CTA partial sums [rep][grid.x][3]
+  int* timeout;           // set when a bounded wait on a cluster exchange gave up
   const cplx<T>* tw;      // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
   int flags;
@@ -77,33 +97,77 @@ __device__ __forceinline__ void cluster_sync() {
   }
 }
 
-// Store into element ``off`` of the CTA-``rank`` copy of shared array ``buf``
-// (st.shared::cluster on the address mapa gives for that rank).
+// shared::cluster address of ``p`` in the copy of this CTA's shared memory
+// that belongs to cluster rank ``rank``
 __device__ __forceinline__ uint32_t dsmem_map(const void* p, int rank) {
   const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(p));
   uint32_t r;
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
   return r;
 }
-__device__ __forceinline__ void st_dsmem_raw(uint32_t a, float2 v) {
-  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(a), "f"(v.x), "f"(v.y) : "memory");
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
-__device__ __forceinline__ void st_dsmem_raw(uint32_t a, double2 v) {
-  asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(a), "d"(v.x), "d"(v.y) : "memory");
-}
-__device__ __forceinline__ void st_dsmem_raw(uint32_t a, float v) {
-  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(a), "f"(v) : "memory");
-}
-__device__ __forceinline__ void st_dsmem_raw(uint32_t a, double v) {
-  asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(a), "d"(v) : "memory");
-}
-template <int CL, typename V>
-__device__ __forceinline__ void st_dsmem(V* buf, int rank, int off, V val) {
-  if constexpr (CL == 1) {
-    buf[off] = val;
-  } else {
-    st_dsmem_raw(dsmem_map(buf + off, rank), val);
+
+// Cluster exchange state: send / receive block arrays, two mbarriers (one per
+// exchange direction) and their phase parities.
+template <typename T>
+struct Xchg {
+  cplx<T>* sb;
+  cplx<T>* rb;
+  uint64_t* mbar;
+  uint32_t phases;
+  int* timeout;
+};
+
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* mbar, uint32_t parity, int* timeout) {
+  const uint32_t a = smem_u32(mbar);
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return;
+    if (clock64() - t0 > (1ll << 31)) {  // about a second: give up, flag it, keep the cluster in step
+      atomicExch(timeout, 1);
+      return;
+    }
   }
+}
+
+// Every thread has written its share of the send blocks; copy block d to CTA d
+// (cp.async.bulk shared::cta -> shared::cluster, completing on the receiver's
+// mbarrier ``which``) and wait until all CL incoming blocks have landed.
+template <typename T, int CL>
+__device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, int blk) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  cluster_sync<CL, true>();  // send blocks complete here, receive blocks free everywhere
+  if (threadIdx.x == 0) {
+    const uint32_t bytes = uint32_t(blk * sizeof(cplx<T>));
+    const uint32_t mb = smem_u32(&x.mbar[which]);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes * CL) : "memory");
+    for (int d = 0; d < CL; ++d) {
+      const uint32_t dst = dsmem_map(x.rb + size_t(rank) * blk, d);
+      const uint32_t src = smem_u32(x.sb + size_t(d) * blk);
+      const uint32_t rmb = dsmem_map(&x.mbar[which], d);
+      asm volatile(
+          "cp.async.bulk.shared::cluster.shared::cta.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+          "r"(src), "r"(bytes), "r"(rmb)
+          : "memory");
+    }
+    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+  }
+  mbar_wait_bounded(&x.mbar[which], (x.phases >> which) & 1u, x.timeout);
+  x.phases ^= 1u << which;
+}
+
+// The send blocks may be rewritten once this CTA's outgoing copies read them.
+__device__ __forceinline__ void send_blocks_free() {
+  if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+  __syncthreads();
 }
 
 // z (or y) position of FFT index n in the Makhoul even/odd permutation
@@ -122,27 +186,6 @@ __device__ __forceinline__ cplx<T> dct3_pre(const cplx<T>* L, int i, const cplx<
   cplx<T> w = dtw[i];
   w.y = -w.y;
   return cmul<T>(u, w);
-}
-
-// first-pass input of the two-row C2R: Z = X_a + i X_b with Hermitian extension;
-// slot 0 of each half holds (X[0], X[N/2]) packed.
-template <typename T, int N>
-__device__ __forceinline__ cplx<T> c2r_pre(const cplx<T>* L, int i) {
-  if (i == 0) {
-    cplx<T> a = L[pad(0)], b = L[pad(N / 2)];
-    return mk<T>(a.x, b.x);
-  }
-  if (i == N / 2) {
-    cplx<T> a = L[pad(0)], b = L[pad(N / 2)];
-    return mk<T>(a.y, b.y);
-  }
-  if (i < N / 2) {
-    cplx<T> a = L[pad(i)], b = L[pad(N / 2 + i)];
-    return mk<T>(a.x - b.y, a.y + b.x);
-  }
-  const int k = N - i;
-  cplx<T> a = L[pad(k)], b = L[pad(N / 2 + k)];
-  return mk<T>(a.x + b.y, b.x - a.y);
 }
 
 template <typename T, int N, int CL, bool DCT>
@@ -215,8 +258,26 @@ struct PlaneOps {
     }
   }
 
-  // inverse y transform of the owned columns, then scatter into row layout
-  static __device__ void col_inverse_to_rows(cplx<T>* buf, int rank, const TwTables<T>& tw) {
+  // ---- spectral-slot access of the row and column phases ----------------
+  // periodic row phase: slot k of half h (row 2q + h) of row-pair line q
+  static __device__ __forceinline__ const cplx<T>& row_slot(const cplx<T>* lb, const Xchg<T>& x, int q, int h, int k) {
+    if constexpr (CL == 1) return lb[q * LS + pad(h * (N / 2) + k)];
+    else return x.rb[(k / NC) * Cfg::BLK + (2 * q + h) * Cfg::SA + (k % NC)];
+  }
+  // Neumann row phase: slot kz of row-pair line q
+  static __device__ __forceinline__ const cplx<T>& row_pair(const cplx<T>* lb, const Xchg<T>& x, int q, int kz) {
+    if constexpr (CL == 1) return lb[q * LS + pad(kz)];
+    else return x.rb[(kz / (2 * NC)) * Cfg::BLK + q * Cfg::SA + (kz % (2 * NC))];
+  }
+  // forward column phase: element ky of column line c
+  static __device__ __forceinline__ const cplx<T>& col_in(const cplx<T>* lb, const Xchg<T>& x, int c, int ky) {
+    if constexpr (CL == 1) return lb[c * LS + pad(ky)];
+    else return x.rb[(ky / ROWS) * Cfg::BLK + (ky % ROWS) * Cfg::SBs + c];
+  }
+
+  // inverse y transform of the owned columns, then hand each value to the row
+  // phase: in place (CL == 1) or through the cluster exchange
+  static __device__ void col_inverse_to_rows(cplx<T>* buf, Xchg<T>& xs, int rank, const TwTables<T>& tw) {
     const int line = threadIdx.x / G, t = threadIdx.x % G;
     cplx<T>* L = buf + line * LS;
     cplx<T> v[E];
@@ -225,38 +286,77 @@ struct PlaneOps {
     } else {
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return dct3_pre<T, N>(L, i, tw.d); });
     }
-    cluster_sync<CL, false>();
-    const int kc = rank * NC + line;  // global complex column
     constexpr int RL = Cfg::RL_INV;
+    if constexpr (CL == 1) {
+      __syncthreads();
+      const int kc = line;
 #pragma unroll
-    for (int b = 0; b < E / RL; ++b)
+      for (int b = 0; b < E / RL; ++b)
 #pragma unroll
-      for (int r = 0; r < RL; ++r) {
-        const int n = out_index<N, +1>(t, b, r);
-        const cplx<T> val = v[b * RL + r];
-        if constexpr (!DCT) {
-          const int dest = n / ROWS, yl = n % ROWS;
-          st_dsmem<CL>(buf, dest, (yl >> 1) * LS + pad((yl & 1) * (N / 2) + kc), val);
-        } else {
-          const int y = mk_perm<N>(n);
-          const int dest = y / ROWS, yl = y % ROWS;
-          T* rb = reinterpret_cast<T*>(buf);
-          const int base = (yl >> 1) * LS;
-          st_dsmem<CL>(rb, dest, 2 * (base + pad(2 * kc)) + (yl & 1), val.x);
-          st_dsmem<CL>(rb, dest, 2 * (base + pad(2 * kc + 1)) + (yl & 1), val.y);
+        for (int r = 0; r < RL; ++r) {
+          const int n = out_index<N, +1>(t, b, r);
+          const cplx<T> val = v[b * RL + r];
+          if constexpr (!DCT) {
+            buf[(n >> 1) * LS + pad((n & 1) * (N / 2) + kc)] = val;
+          } else {
+            const int y = mk_perm<N>(n);
+            T* rb = reinterpret_cast<T*>(buf);
+            const int base = (y >> 1) * LS;
+            rb[2 * (base + pad(2 * kc)) + (y & 1)] = val.x;
+            rb[2 * (base + pad(2 * kc + 1)) + (y & 1)] = val.y;
+          }
         }
-      }
-    cluster_sync<CL, true>();
+      __syncthreads();
+    } else {
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int n = out_index<N, +1>(t, b, r);
+          const cplx<T> val = v[b * RL + r];
+          if constexpr (!DCT) {
+            const int dest = n / ROWS, yl = n % ROWS;
+            xs.sb[dest * Cfg::BLK + yl * Cfg::SA + line] = val;
+          } else {
+            const int y = mk_perm<N>(n);
+            const int dest = y / ROWS, yl = y % ROWS;
+            T* sb = reinterpret_cast<T*>(xs.sb + dest * Cfg::BLK + (yl >> 1) * Cfg::SA + 2 * line);
+            sb[yl & 1] = val.x;
+            sb[2 + (yl & 1)] = val.y;
+          }
+        }
+      bulk_exchange<T, CL>(xs, 0, rank, Cfg::BLK);
+    }
   }
 
   // ---- row phase -------------------------------------------------------
   // inverse z transform of row pair ``line``; v slot holds psi(y0, z), psi(y0+1, z)
-  static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], cplx<T>* L, int t,
-                                                     const TwTables<T>& tw) {
+  static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], const cplx<T>* buf, const Xchg<T>& xs,
+                                                     cplx<T>* L, int q, int t, const TwTables<T>& tw) {
     if constexpr (!DCT) {
-      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return c2r_pre<T, N>(L, i); });
+      // Z = X_a + i X_b with Hermitian extension; slot 0 holds (X[0], X[N/2])
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
+        if (i == 0 || i == N / 2) {
+          const cplx<T> a = row_slot(buf, xs, q, 0, 0), b = row_slot(buf, xs, q, 1, 0);
+          return i == 0 ? mk<T>(a.x, b.x) : mk<T>(a.y, b.y);
+        }
+        const int k = i < N / 2 ? i : N - i;
+        const cplx<T> a = row_slot(buf, xs, q, 0, k), b = row_slot(buf, xs, q, 1, k);
+        return i < N / 2 ? mk<T>(a.x - b.y, a.y + b.x) : mk<T>(a.x + b.y, b.x - a.y);
+      });
     } else {
-      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return dct3_pre<T, N>(L, i, tw.d); });
+      // REDFT01 input: exp(+i pi i/2N) (X[i] - i X[N-i]), X[N] = 0
+      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
+        const cplx<T> a = row_pair(buf, xs, q, i);
+        cplx<T> u = a;
+        if (i != 0) {
+          const cplx<T> b = row_pair(buf, xs, q, N - i);
+          u = mk<T>(a.x + b.y, a.y - b.x);
+        }
+        cplx<T> w = tw.d[i];
+        w.y = -w.y;
+        return cmul<T>(u, w);
+      });
     }
   }
 
@@ -268,9 +368,10 @@ struct PlaneOps {
     return n;
   }
 
-  // forward z transform from registers, then scatter to column layout
-  static __device__ void row_forward_to_cols(cplx<T> (&v)[E], cplx<T>* buf, cplx<T>* L, int rank, int line, int t,
-                                             const TwTables<T>& tw) {
+  // forward z transform from registers, then hand the spectra to the column
+  // owners (in place or through the cluster exchange)
+  static __device__ void row_forward_to_cols(cplx<T> (&v)[E], cplx<T>* buf, Xchg<T>& xs, cplx<T>* L, int rank,
+                                             int line, int t, const TwTables<T>& tw) {
     fft_regs<T, N, -1>(v, L, t, tw.f);
     constexpr int RL = Cfg::RL_FWD;
     __syncwarp();
@@ -279,7 +380,6 @@ struct PlaneOps {
 #pragma unroll
       for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
     __syncwarp();
-    const int y0 = rank * ROWS + 2 * line;  // global y of the real part
     if constexpr (!DCT) {
       // split Z into the two half spectra; slot k < N/2 from register r < RL/2
       cplx<T> oa[E / 2], ob[E / 2];
@@ -299,17 +399,33 @@ struct PlaneOps {
             ob[s] = mk<T>(T(0.5) * (zk.y + zm.y), T(0.5) * (zm.x - zk.x));
           }
         }
-      cluster_sync<CL, false>();
+      if constexpr (CL == 1) {
+        __syncthreads();
+        const int y0 = 2 * line;
 #pragma unroll
-      for (int b = 0; b < E / RL; ++b)
+        for (int b = 0; b < E / RL; ++b)
 #pragma unroll
-        for (int r = 0; r < RL / 2; ++r) {
-          const int k = out_index<N, -1>(t, b, r);
-          const int s = b * (RL / 2) + r;
-          const int col = (k % NC) * LS;
-          st_dsmem<CL>(buf, k / NC, col + pad(y0), oa[s]);
-          st_dsmem<CL>(buf, k / NC, col + pad(y0 + 1), ob[s]);
-        }
+          for (int r = 0; r < RL / 2; ++r) {
+            const int k = out_index<N, -1>(t, b, r);
+            const int s = b * (RL / 2) + r;
+            buf[k * LS + pad(y0)] = oa[s];
+            buf[k * LS + pad(y0 + 1)] = ob[s];
+          }
+        __syncthreads();
+      } else {
+        send_blocks_free();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL / 2; ++r) {
+            const int k = out_index<N, -1>(t, b, r);
+            const int s = b * (RL / 2) + r;
+            cplx<T>* blk = xs.sb + (k / NC) * Cfg::BLK + (k % NC);
+            blk[(2 * line) * Cfg::SBs] = oa[s];
+            blk[(2 * line + 1) * Cfg::SBs] = ob[s];
+          }
+        bulk_exchange<T, CL>(xs, 1, rank, Cfg::BLK);
+      }
     } else {
       cplx<T> o[E];
 #pragma unroll
@@ -322,31 +438,45 @@ struct PlaneOps {
           cplx<T> bm = cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w));
           o[b * RL + r] = cadd<T>(a, bm);
         }
-      cluster_sync<CL, false>();
+      if constexpr (CL == 1) {
+        __syncthreads();
+        const int y0 = 2 * line;
 #pragma unroll
-      for (int b = 0; b < E / RL; ++b)
+        for (int b = 0; b < E / RL; ++b)
 #pragma unroll
-        for (int r = 0; r < RL; ++r) {
-          const int k = out_index<N, -1>(t, b, r);
-          const int p = k >> 1;
-          T* rb = reinterpret_cast<T*>(buf);
-          const int col = 2 * (p % NC) * LS;
-          st_dsmem<CL>(rb, p / NC, col + 2 * pad(y0) + (k & 1), o[b * RL + r].x);
-          st_dsmem<CL>(rb, p / NC, col + 2 * pad(y0 + 1) + (k & 1), o[b * RL + r].y);
-        }
+          for (int r = 0; r < RL; ++r) {
+            const int k = out_index<N, -1>(t, b, r);
+            T* cb = reinterpret_cast<T*>(buf + (k >> 1) * LS);
+            cb[2 * pad(y0) + (k & 1)] = o[b * RL + r].x;
+            cb[2 * pad(y0 + 1) + (k & 1)] = o[b * RL + r].y;
+          }
+        __syncthreads();
+      } else {
+        send_blocks_free();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) {
+            const int k = out_index<N, -1>(t, b, r);
+            const int p = k >> 1;
+            T* blk = reinterpret_cast<T*>(xs.sb + (p / NC) * Cfg::BLK + (p % NC));
+            blk[2 * (2 * line) * Cfg::SBs + (k & 1)] = o[b * RL + r].x;
+            blk[2 * (2 * line + 1) * Cfg::SBs + (k & 1)] = o[b * RL + r].y;
+          }
+        bulk_exchange<T, CL>(xs, 1, rank, Cfg::BLK);
+      }
     }
-    cluster_sync<CL, true>();
   }
 
   // ---- column phase, forward direction ---------------------------------
-  static __device__ void col_forward_store(cplx<T>* buf, cplx<T>* __restrict__ plane, int rank,
+  static __device__ void col_forward_store(cplx<T>* buf, const Xchg<T>& xs, cplx<T>* __restrict__ plane, int rank,
                                            const TwTables<T>& tw) {
     const int line = threadIdx.x / G, t = threadIdx.x % G;
     cplx<T>* L = buf + line * LS;
     cplx<T> v[E];
     constexpr int RL = Cfg::RL_FWD;
     if constexpr (!DCT) {
-      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(i)]; });
+      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return col_in(buf, xs, line, i); });
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
@@ -378,7 +508,7 @@ struct PlaneOps {
         __syncthreads();
       }
     } else {
-      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(mk_perm<N>(i))]; });
+      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return col_in(buf, xs, line, mk_perm<N>(i)); });
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
@@ -463,6 +593,21 @@ plane_kernel(PlaneArgs<T> a) {
 
   int rank = 0;
   if constexpr (CL > 1) rank = int(cg::this_cluster().block_rank());
+  Xchg<T> xs{};
+  if constexpr (CL > 1) {
+    xs.sb = reinterpret_cast<cplx<T>*>(smem_raw + Cfg::SB_OFF);
+    xs.rb = reinterpret_cast<cplx<T>*>(smem_raw + Cfg::RB_OFF);
+    xs.mbar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::MB_OFF);
+    xs.phases = 0;
+    xs.timeout = a.timeout;
+    if (threadIdx.x == 0) {
+      // peers see the initialised barriers after the cluster barrier that opens
+      // the first exchange
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[0])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[1])) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+  }
   const int x = blockIdx.x / CL;
   const int rep = blockIdx.y;
   const int line = threadIdx.x / G, t = threadIdx.x % G;
@@ -474,8 +619,8 @@ plane_kernel(PlaneArgs<T> a) {
 
   if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi) {
     Ops::col_load(buf, a.src + plane_off, rank);
-    Ops::col_inverse_to_rows(buf, rank, tw);
-    Ops::row_inverse(v, L, t, tw);
+    Ops::col_inverse_to_rows(buf, xs, rank, tw);
+    Ops::row_inverse(v, buf, xs, L, line, t, tw);
 
     if (a.flags & (kFlPsiOut | kFlL1 | kFlEnergy)) {
       KahanSum s0, s1, s2;
@@ -514,8 +659,8 @@ plane_kernel(PlaneArgs<T> a) {
     }
     if constexpr (MODE == kPlaneStep) {
       row_nonlin<T, N, CL, DCT>(v, L, t, a.pp);
-      Ops::row_forward_to_cols(v, buf, L, rank, line, t, tw);
-      Ops::col_forward_store(buf, a.dst + plane_off, rank, tw);
+      Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
+      Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
     }
   } else {  // kPlaneInit: real psi -> partial spectra of psi (dst2) and N(psi) (dst)
     const double* src = a.psi_in + real_off;
@@ -543,9 +688,13 @@ plane_kernel(PlaneArgs<T> a) {
           }
           v[b * R0 + r] = mk<T>(pa, pb);
         }
-      Ops::row_forward_to_cols(v, buf, L, rank, line, t, tw);
-      Ops::col_forward_store(buf, (field == 0 ? a.dst2 : a.dst) + plane_off, rank, tw);
+      Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
+      Ops::col_forward_store(buf, xs, (field == 0 ? a.dst2 : a.dst) + plane_off, rank, tw);
     }
+  }
+  if constexpr (CL > 1) {
+    // outgoing copies must have finished reading this CTA's send blocks
+    if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 }
 

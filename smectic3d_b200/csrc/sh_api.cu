@@ -160,7 +160,7 @@ int sh_create(const sh_params* p, sh_handle** out) {
     s->err = cudaGetErrorString(e);
     return bad("stream");
   }
-  if ((e = cudaMalloc(&s->d_flag, sizeof(int))) != cudaSuccess ||
+  if ((e = cudaMalloc(&s->d_flag, 2 * sizeof(int))) != cudaSuccess ||
       (e = cudaMalloc(&s->d_psi, n3 * p->batch * sizeof(double))) != cudaSuccess ||
       (e = cudaMalloc(&s->d_eps, p->batch * sizeof(double))) != cudaSuccess ||
       (e = cudaMalloc(&s->d_scalar, p->batch * sizeof(double))) != cudaSuccess) {
@@ -176,7 +176,7 @@ int sh_create(const sh_params* p, sh_handle** out) {
     g_err = std::string("device allocation: ") + cudaGetErrorString(e);
     return SH_ENOMEM;
   }
-  cudaMemset(s->d_flag, 0, sizeof(int));
+  cudaMemset(s->d_flag, 0, 2 * sizeof(int));
   cudaMemcpy(s->d_eps, s->eps.data(), p->batch * sizeof(double), cudaMemcpyHostToDevice);
   s->l1_last.assign(p->batch, 0.0);
   int rc = s->setup();
@@ -204,7 +204,7 @@ int sh_set_psi_device(sh_handle* h, const double* dev_psi) {
   if (dev_psi != s->d_psi)
     API_CUDA(h, cudaMemcpyAsync(s->d_psi, dev_psi, s->n3() * s->p.batch * sizeof(double), cudaMemcpyDeviceToDevice,
                                 s->stream));
-  API_CUDA(h, cudaMemsetAsync(s->d_flag, 0, sizeof(int), s->stream));
+  API_CUDA(h, cudaMemsetAsync(s->d_flag, 0, 2 * sizeof(int), s->stream));
   return s->init_from_psi();
 }
 
@@ -267,8 +267,8 @@ int sh_step(sh_handle* h, int nsteps) {
   int rc = sh_step_async(h, nsteps);
   if (rc) return rc;
   SolverBase* s = h->s;
-  int flag = 0;
-  API_CUDA(h, cudaMemcpyAsync(&flag, s->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+  int flag[2] = {0, 0};
+  API_CUDA(h, cudaMemcpyAsync(flag, s->d_flag, 2 * sizeof(int), cudaMemcpyDeviceToHost, s->stream));
   if (s->p.energy_trace && nsteps > 0) {
     const size_t old = s->energy_trace.size();
     s->energy_trace.resize(old + size_t(nsteps) * s->p.batch);
@@ -279,7 +279,8 @@ int sh_step(sh_handle* h, int nsteps) {
     API_CUDA(h, cudaMemcpyAsync(s->l1_last.data(), s->d_scalar, s->p.batch * sizeof(double), cudaMemcpyDeviceToHost,
                                 s->stream));
   API_CUDA(h, cudaStreamSynchronize(s->stream));
-  if (flag) return fail(h, SH_ENONFINITE, "psi became non-finite");
+  if (flag[1]) return fail(h, SH_ETIMEOUT, "a cluster exchange wait gave up (results invalid)");
+  if (flag[0]) return fail(h, SH_ENONFINITE, "psi became non-finite");
   return SH_OK;
 }
 

@@ -33,7 +33,7 @@ struct SolverBase {
   std::string err;
   long long steps = 0;
   long long launches = 0;
-  int* d_flag = nullptr;
+  int* d_flag = nullptr;       // [0] non-finite state, [1] cluster-exchange timeout
   double* d_psi = nullptr;     // batch * N^3 doubles (dense)
   double* d_stash = nullptr;   // L1 reference psi
   double* d_eps = nullptr;
@@ -192,6 +192,7 @@ struct Solver final : SolverBase {
     a.tw = tw;
     a.pp = point_params();
     a.red = d_red_plane;
+    a.timeout = d_flag + 1;
     return a;
   }
   PencilArgs<T> pencil_args() const {
