@@ -119,6 +119,36 @@ int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kga
 int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes);
 int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes);
 
+/*
+ * L1 monitor of two device psi fields that allocates no device memory.
+ * No counterpart in the reference: it is the monitor of sh_l1 (the
+ * reference's L1 of periodicFFT/pf3d.cpp:489-509, evaluated on caller
+ * buffers) for callers that must not let a library allocate. Examples: a host
+ * that manages all device memory through its own pool, code running while a
+ * stream is captured into a CUDA graph (cudaMalloc/cudaFree are not allowed
+ * there), and real-time loops that cannot take the implicit device
+ * synchronisation of cudaMalloc/cudaFree.
+ *
+ * dev_psi_new, dev_psi_old: batch*n3 doubles each on the current device.
+ * dev_out: batch doubles on the current device; receives
+ * sum|new - old| / (dt sum|new|) per replica.
+ * stream: a cudaStream_t; the call is stream-ordered and returns without
+ * synchronising.
+ *
+ * The per-block partial sums go into one fixed device array of the library
+ * (256 KiB, held by every GPU that loads the library until the process
+ * exits). batch is therefore at most SH_L1_NOALLOC_MAX_BATCH; larger values
+ * return SH_EINVAL. The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress) with the device current. Make that first call
+ * before any stream capture. Each call overwrites every slot it reads, so no
+ * state carries over between calls. Calls that overlap on the GPU (on
+ * different streams, or on several host threads) share the array and race.
+ * Errors: sh_last_error(NULL).
+ */
+#define SH_L1_NOALLOC_MAX_BATCH 128
+int sh_l1_noalloc(const double* dev_psi_new, const double* dev_psi_old, long long n3, int batch, double dt,
+                  double* dev_out, void* stream);
+
 /* Pinned host memory for fast host<->device copies. */
 int sh_host_alloc(size_t bytes, void** out);
 int sh_host_free(void* p);

@@ -23,7 +23,7 @@ EXPORTS = (
     "sh_default_params", "sh_create", "sh_destroy", "sh_set_psi", "sh_set_psi_device", "sh_get_psi",
     "sh_get_psi_device", "sh_step", "sh_step_async", "sh_run", "sh_energy", "sh_energy_trace", "sh_l1",
     "sh_surface_step", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
-    "sh_profile_steps", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
+    "sh_l1_noalloc", "sh_profile_steps", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
 )
 
 
@@ -76,6 +76,7 @@ def load() -> C.CDLL:
         "sh_checkpoint_load": (C.c_int, [vp, vp, C.c_size_t]),
         "sh_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),
         "sh_host_free": (C.c_int, [vp]),
+        "sh_l1_noalloc": (C.c_int, [vp, vp, C.c_longlong, C.c_int, C.c_double, vp, vp]),
         "sh_profile_steps": (C.c_int, [vp, C.c_int, dp, dp]),
         "sh_synchronize": (C.c_int, [vp]),
         "sh_stream": (vp, [vp]),

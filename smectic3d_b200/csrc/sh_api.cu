@@ -15,6 +15,10 @@ struct sh_handle {
 static thread_local std::string g_err;
 
 namespace shb {
+void set_global_error(const std::string& msg) { g_err = msg; }
+}  // namespace shb
+
+namespace shb {
 
 __global__ void finalize_kernel(const double* red_plane, int nbp, const double* red_spec, int nbs, int what,
                                 double dv, double spec_norm, double alpha, double dt, double* out) {
