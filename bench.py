@@ -194,6 +194,22 @@ def run_ours(args, rank, world, local_rank, dist):
     rel_err = float(np.linalg.norm(a32 - a64) / max(np.linalg.norm(a64 if prec == "fp32" else a32), 1e-300))
     s64.close()
 
+    # ---- accuracy of the FP32 path after 100 steps (the north-star check),
+    # on the workload's IC and on the non-decaying reference-amplitude lamellae
+    acc100 = {}
+    for label, ic0 in (("workload_ic", psi0),
+                       ("lamellae_amp1.3", S.ic.undulated_lamellae(n, p32.dx, amp=1.3, seed=rank)
+                        if batch == 1 else None)):
+        if ic0 is None:
+            continue
+        outs = {}
+        for pr in ("fp32", "fp64"):
+            with S.Solver(params_for(args.workload, pr)) as sv:
+                sv.set_psi(ic0)
+                sv.step(100)
+                outs[pr] = sv.get_psi()
+        acc100[label] = float(np.linalg.norm(outs["fp32"] - outs["fp64"]) / np.linalg.norm(outs["fp64"]))
+
     # ---- per-pass device times (roofline of the dominant kernel) -----------
     nprof = max(10, min(200, k // 10))
     ms_pencil, ms_plane = s32.profile_steps(nprof)
@@ -234,6 +250,8 @@ def run_ours(args, rank, world, local_rank, dist):
            "h2d_bytes_per_step": nbytes / k, "d2h_bytes_per_step": (nbytes + 8 * batch * (k // 100) + 4) / k,
            "api": "smectic3d_b200.Solver.run -> sh_run (pinned host psi in, K steps with the L1 monitor every 100, psi out)"}
 
+    adj = adjoint_ratio(args, torch) if args.adjoint_steps > 0 else None
+
     if rank != 0:
         return None
     cpu = cpu_baseline(args.workload, budget_s=args.cpu_seconds) if world == 1 else None
@@ -258,10 +276,43 @@ def run_ours(args, rank, world, local_rank, dist):
         "clocks": clk,
         "other_precision": {"precision": other, "value": world * k / (ms64 / 1e3), "ms_per_step": ms64 / k,
                             "speedup_fp32_over_fp64": (ms64 / ms) if prec == "fp32" else (ms / ms64),
-                            "rel_err_fp32_vs_fp64": rel_err, "after_steps": w + k},
-        "adjoint_forward_ratio": None,
+                            "rel_err_fp32_vs_fp64": rel_err, "after_steps": w + k,
+                            "rel_err_fp32_vs_fp64_after_100_steps": acc100},
+        "adjoint_forward_ratio": adj["backward_over_forward"] if adj else None,
+        "adjoint": adj,
     }
     return line
+
+
+def adjoint_ratio(args, torch):
+    """Differentiation workload: 128^3 periodic, FP32 forward, FP64 gradient
+    accumulation, dt=0.05, checkpoints every 50 steps, L = 1/2 ||psi_T - target||^2
+    with target 0.5 cos(1.05 z).  Times T forward steps and sh_adjoint over the
+    same T steps (its own forward sweep, the recompute and the reverse sweep)."""
+    import numpy as np
+    import smectic3d_b200 as S
+    n, k = 128, 50
+    t_steps = args.adjoint_steps
+    p = S.Params(n=n, precision="fp32", dt=0.05, eps=-0.75)
+    psi0 = S.ic.noise(n, 0)
+    target = 0.5 * np.broadcast_to(np.cos(1.05 * np.arange(n) * p.dx)[None, None, :], (n, n, n))
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(5)
+        s.set_psi(psi0)
+        s.synchronize()
+        t0 = time.perf_counter()
+        s.step(t_steps)
+        t_fwd = time.perf_counter() - t0
+        lam = s.get_psi() - target
+        s.adjoint(psi0, 10, lam, ckpt_every=5)  # warm the adjoint kernels
+        t0 = time.perf_counter()
+        ge, gq, _ = s.adjoint(psi0, t_steps, lam, ckpt_every=k)
+        t_adj = time.perf_counter() - t0
+    return {"workload": f"periodic {n}^3 fp32, dt=0.05, T={t_steps}, checkpoints every {k}",
+            "forward_ms_per_step": t_fwd / t_steps * 1e3, "adjoint_ms_per_step": t_adj / t_steps * 1e3,
+            "total_over_forward": t_adj / t_fwd, "backward_over_forward": (t_adj - t_fwd) / t_fwd,
+            "grad_eps": float(ge[0]), "grad_q0": float(gq[0])}
 
 
 # ---------------------------------------------------------------------------
@@ -328,6 +379,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="neumann256", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--adjoint-steps", type=int, default=200, help="steps of the adjoint ratio (0 = skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

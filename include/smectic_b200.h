@@ -114,6 +114,17 @@ int sh_l1(sh_handle* h, double* out, int* count);
  * N*N values per replica: z index (or -1), v_n, H, K (NaN where no crossing). */
 int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kgauss);
 
+/* Discrete adjoint of the CNAB2 loop (plain periodic step, SH_CNAB2, no
+ * advection or penalty).  Integrates `nsteps` steps from psi0, then runs the
+ * reverse sweep for a loss L whose gradient with respect to psi^T is
+ * dl_dpsi_t (e.g. psi^T - target for 1/2 ||psi^T - target||^2), recomputing
+ * the forward states from checkpoints taken every `ckpt_every` steps.
+ * Outputs per replica: dL/d eps, dL/d q0 (FP64 accumulation) and dL/d psi0
+ * (batch*N^3).  No counterpart in the reference (BASELINE differentiation
+ * addition); the forward pass is the reference loop (periodicFFT/pf3dVal.cpp:270-301). */
+int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every,
+               double* g_eps, double* g_q0, double* g_psi0);
+
 /* Binary checkpoint of the full state (including the AB2 history, which the
  * reference's text files drop): query size with buf == NULL. */
 int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes);

@@ -1,0 +1,90 @@
+"""Autotuner for the plane-pass cluster size.
+
+Each built shape offers a few cluster sizes for the plane pass (``variant``):
+- CL = 1 and 2 at 64^3;
+- CL = 1, 2 and 4 at 128^3;
+- CL = 4, 8 and 16 at 256^3.
+
+The tuner times a few steps of every built candidate for a given (n, batch,
+boundary, precision, advection) and keeps the fastest. Results are cached in a
+JSON file keyed by that tuple and by the GPU name, under
+$SMECTIC_B200_CACHE (default ~/.cache/smectic3d_b200/tuned.json).
+"""
+from __future__ import annotations
+
+import dataclasses
+import json
+import os
+import time
+from pathlib import Path
+
+import numpy as np
+
+CANDIDATES = {16: (1,), 32: (1,), 64: (1, 2), 128: (1, 2, 4), 256: (4, 8, 16), 512: (16,)}
+
+
+def cache_path() -> Path:
+    base = os.environ.get("SMECTIC_B200_CACHE")
+    if base:
+        return Path(base)
+    return Path.home() / ".cache" / "smectic3d_b200" / "tuned.json"
+
+
+def _key(p, gpu: str) -> str:
+    return f"{gpu}|n={p.n}|b={p.batch}|{p.boundary}|{p.precision}|adv={int(bool(p.advection))}"
+
+
+def _gpu_name() -> str:
+    try:
+        import torch
+        return torch.cuda.get_device_name(0)
+    except Exception:
+        return "unknown"
+
+
+def _time_variant(p, variant: int, steps: int) -> float:
+    from .solver import Solver
+    q = dataclasses.replace(p, variant=variant, energy_trace=False, l1_interval=0)
+    with Solver(q) as s:
+        shape = (q.batch, q.n, q.n, q.n) if q.batch > 1 else (q.n, q.n, q.n)
+        s.set_psi(np.random.default_rng(0).uniform(-0.1, 0.1, size=shape))
+        s.step(2)
+        s.synchronize()
+        t0 = time.perf_counter()
+        s.step(steps)
+        t1 = time.perf_counter()
+    return (t1 - t0) / steps
+
+
+def tune(p, steps: int = 20, use_cache: bool = True) -> dict:
+    """Time every built cluster size of ``p``'s shape; returns
+    {"variant": best, "us_per_step": {variant: us}} and caches it."""
+    gpu = _gpu_name()
+    key = _key(p, gpu)
+    path = cache_path()
+    cache = {}
+    if path.exists():
+        try:
+            cache = json.loads(path.read_text())
+        except ValueError:
+            cache = {}
+    if use_cache and key in cache:
+        return cache[key]
+    times = {}
+    for v in CANDIDATES.get(p.n, (0,)):
+        try:
+            times[v] = _time_variant(p, v, steps) * 1e6
+        except Exception:  # not built for this precision / shared memory
+            continue
+    if not times:
+        raise RuntimeError(f"no plane-pass variant runs for {key}")
+    best = min(times, key=times.get)
+    rec = {"variant": best, "us_per_step": {str(k): v for k, v in times.items()}}
+    cache[key] = rec
+    path.parent.mkdir(parents=True, exist_ok=True)
+    path.write_text(json.dumps(cache, indent=1, sort_keys=True))
+    return rec
+
+
+def best_variant(p) -> int:
+    return int(tune(p)["variant"])

@@ -19,7 +19,23 @@
 
 namespace shb {
 
-enum PencilMode : int { kPencilStep = 0, kPencilInit = 1, kPencilEnergy = 2 };
+enum PencilMode : int {
+  kPencilStep = 0,
+  kPencilInit = 1,
+  kPencilEnergy = 2,
+  kPencilStepAdv = 3,  // step that also emits the partials of i q_x psihat and opSH psihat
+  kPencilInitAdv = 4,
+  kPencilStokes = 5,   // Stokes velocity from the stress (periodicFFT/pf3d.cpp:433-447)
+  kPencilXMul = 6,     // partial P -> partial of i q_x times its spectrum (second x derivative of psi)
+  kPencilSpec = 7,     // partial P -> psihat, pencil-major
+  kPencilAdjInit = 8,  // adjoint: partial of lambda^T -> lambdahat^T, mu partial
+  kPencilAdj = 9,      // adjoint step: lambdahat^n = A lambdahat^{n+1} + ghat^n, mu partial, parameter gradients
+  kPencilAdjOut = 10,  // adjoint: lambdahat -> its x-inverse partial (for lambda^0 in real space)
+};
+// line sets of shared memory a pencil mode uses (FFT scratch, stash, Stokes components)
+__host__ __device__ constexpr int pencil_sets(int mode) {
+  return mode == kPencilStokes ? 3 : ((mode == kPencilStepAdv || mode == kPencilInitAdv) ? 2 : 1);
+}
 
 template <typename T, int N, bool DCT>
 struct PencilCfg {
@@ -31,9 +47,10 @@ struct PencilCfg {
   static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
   static constexpr int TILES = FP / TK;
   static constexpr int RL = radix_of<N, -1, Plan<N>::P - 1>();
-  static constexpr size_t TW_OFF = size_t(TK) * LS * sizeof(cplx<T>);
-  static constexpr size_t RED_OFF = TW_OFF + size_t(tw_total<N>()) * sizeof(cplx<T>);
-  static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
+  static constexpr size_t SET_BYTES = size_t(TK) * LS * sizeof(cplx<T>);
+  static constexpr size_t tw_off(int mode) { return SET_BYTES * pencil_sets(mode); }
+  static constexpr size_t red_off(int mode) { return tw_off(mode) + size_t(tw_total<N>()) * sizeof(cplx<T>); }
+  static constexpr size_t smem(int mode) { return red_off(mode) + 64 * sizeof(double); }
   static_assert(FP % TK == 0, "tile must divide the plane");
   static_assert(THREADS % 32 == 0, "pencil CTA must be whole warps");
 };
@@ -44,6 +61,13 @@ struct PencilArgs {
   const cplx<T>* src2;  // init: partial of N(psi)
   cplx<T>* w;           // state W [rep][FP][N]
   cplx<T>* dst;         // partial of scale * psihat^{n+1}, x-inverse applied [rep][x][FP]
+  cplx<T>* dst_x;       // advection: partial of scale * i q_x psihat^{n+1}
+  cplx<T>* dst_sh;      // advection: partial of scale * opSH psihat^{n+1}
+  cplx<T>* spec_out;     // kFlSpecOut / kPencilSpec: psihat, pencil-major
+  const cplx<T>* spec_a; // adjoint: psihat^n, pencil-major
+  const cplx<T>* spec_b; // adjoint: psihat^{n+1}, pencil-major
+  const cplx<T>* s3[3]; // Stokes: partial stress components (forward y,z applied)
+  cplx<T>* u3[3];       // Stokes: partial velocity components (may alias s3)
   double* red;          // per-CTA spectral energy partial [rep][grid.x]
   int* nonfinite;       // set to 1 when a new coefficient is NaN/Inf
   const T* q;           // wavenumber table (N entries)
@@ -174,9 +198,9 @@ pencil_kernel(PencilArgs<T> a) {
   constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
-  double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::RED_OFF);
+  double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::red_off(MODE));
   const TwTables<T> tw =
-      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS);
+      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::tw_off(MODE)), a.tw, threadIdx.x, Cfg::THREADS);
 
   const int f0 = blockIdx.x * TK;
   const int rep = blockIdx.y;
@@ -208,7 +232,7 @@ pencil_kernel(PencilArgs<T> a) {
   KahanSum acc;
   const bool want_energy = (a.flags & kFlEnergy) != 0;
 
-  if constexpr (MODE == kPencilStep) {
+  if constexpr (MODE == kPencilStep || MODE == kPencilStepAdv) {
     Ops::load_tile(buf, a.src + plane_base, f0);
     // the state W of this line, fetched while the transform runs
     cplx<T> wreg[E];
@@ -277,6 +301,7 @@ pencil_kernel(PencilArgs<T> a) {
           }
         }
         bad |= !isfinite(pn.x) || !isfinite(pn.y);
+        if (a.flags & kFlSpecOut) a.spec_out[(size_t(rep) * FP + f) * N + kx] = pn;
         wrow[kx] = wv;
         v[b * RL + r] = cscale<T>(pn, scale);
       }
@@ -308,7 +333,144 @@ pencil_kernel(PencilArgs<T> a) {
           acc.add(wxy * ((kz == 0 ? 0.5 : 1.0) * d0 * d0 * px * px + d1 * d1 * py * py));
         }
       }
-  } else {  // kPencilInit: W^0 from psi^0 and N(psi^0); P^0 from psi^0
+  } else if constexpr (MODE == kPencilSpec || MODE == kPencilAdjInit || MODE == kPencilAdj) {
+    Ops::load_tile(buf, a.src + plane_base, f0);
+    cplx<T> lreg[E];
+    if constexpr (MODE == kPencilAdj) {
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) lreg[b * RL + r] = wrow[out_index<N, -1>(t, b, r)];
+    }
+    __syncthreads();
+    Ops::forward(v, L, t, tw);
+    if constexpr (MODE == kPencilSpec) {
+      // P = IDFT_x(scale psihat): its forward x transform is N scale psihat
+      const T inv = T(1.0 / (a.pp.scale * N));
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r)
+          a.spec_out[(size_t(rep) * FP + f) * N + out_index<N, -1>(t, b, r)] = cscale<T>(v[b * RL + r], inv);
+    } else if constexpr (!DCT) {
+      // Discrete adjoint of CNAB2 (reverse of psi^{n+1} = A psi^n + B (3 N^n - N^{n-1})):
+      //   lambdahat^n = A lambdahat^{n+1} + ghat^n,  mu^n = B lambda^n,
+      //   dL/dtheta += <lambda^{n+1}, F^-1[dt/2 (psihat^n + psihat^{n+1}) / C2 da/dtheta]>
+      const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha), h = T(0.5 * a.pp.dt);
+      const T qyz = qy * qy + qz0 * qz0;
+      const double wgt = ((kz == 0 || kz == N / 2) ? 1.0 : 2.0) / (double(N) * N * N);
+      const double dadq0 = 4.0 * a.pp.alpha * a.pp.q0;
+      KahanSum ge, gq;
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int kx = out_index<N, -1>(t, b, r);
+          const T qx = __ldg(&a.q[kx]);
+          const T mq2 = qx * qx + qyz;
+          const T d = mq2 - q02;
+          const T al = eps - alpha * d * d;
+          const T inv2 = rcp_rn(T(1) - h * al);
+          const T am = (T(1) + h * al) * inv2, bm = h * inv2;
+          cplx<T> lam = v[b * RL + r];
+          if constexpr (MODE == kPencilAdj) {
+            const cplx<T> l1 = lreg[b * RL + r];
+            const size_t sidx = (size_t(rep) * FP + f) * N + kx;
+            const cplx<T> pa = a.spec_a[sidx], pb = a.spec_b[sidx];
+            const double dx = double(h) * (double(pa.x) + double(pb.x)) * double(inv2);
+            const double dy = double(h) * (double(pa.y) + double(pb.y)) * double(inv2);
+            const double inner = wgt * (double(l1.x) * dx + double(l1.y) * dy);
+            ge.add(inner);
+            gq.add(inner * dadq0 * double(d));
+            lam = mk<T>(am * l1.x + lam.x, am * l1.y + lam.y);
+          }
+          wrow[kx] = lam;
+          v[b * RL + r] = cscale<T>(lam, scale * bm);
+        }
+      if constexpr (MODE == kPencilAdj) {
+        const double te = block_sum(ge.s, scratch);
+        const double tq = block_sum(gq.s, scratch);
+        if (threadIdx.x == 0) {
+          a.red[(size_t(rep) * gridDim.x + blockIdx.x) * 2 + 0] = te;
+          a.red[(size_t(rep) * gridDim.x + blockIdx.x) * 2 + 1] = tq;
+        }
+      }
+    }
+  } else if constexpr (MODE == kPencilAdjOut) {
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) v[b * RL + r] = cscale<T>(wrow[out_index<N, -1>(t, b, r)], scale);
+  } else if constexpr (MODE == kPencilXMul) {
+    Ops::load_tile(buf, a.src + plane_base, f0);
+    __syncthreads();
+    Ops::forward(v, L, t, tw);
+    // P is x-inverse of (scale X); forward x gives N scale X: multiply by i q_x / N
+    const T invn = T(1) / T(N);
+#pragma unroll
+    for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const T qx = __ldg(&a.q[out_index<N, -1>(t, b, r)]) * invn;
+        const cplx<T> val = v[b * RL + r];
+        v[b * RL + r] = mk<T>(-qx * val.y, qx * val.x);
+      }
+  } else if constexpr (MODE == kPencilStokes) {
+    if constexpr (!DCT) {
+      // S -> u = scale CM1 (S - CM2 (q.S)),  CM1 = 1/(rho eta |q|^2), CM2 = q/|q|^2, both 0 at q = 0
+      cplx<T>* set[3] = {buf, buf + TK * LS, buf + 2 * TK * LS};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Ops::load_tile(set[c], a.s3[c] + plane_base, f0);
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cplx<T>* Lc = set[c] + line * LS;
+        Ops::forward(v, Lc, t, tw);
+        __syncwarp();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) Lc[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
+      }
+      __syncwarp();
+      const T ce = T(1.0 / a.pp.eta_rho);
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int kx = out_index<N, -1>(t, b, r);
+          const T qx = __ldg(&a.q[kx]);
+          const T mq2 = qx * qx + qy * qy + qz0 * qz0;
+          const int o = line * LS + pad(kx);
+          const cplx<T> sx = set[0][o], sy = set[1][o], sz = set[2][o];
+          cplx<T> ux = mk<T>(T(0), T(0)), uy = ux, uz = ux;
+          if (mq2 != T(0)) {
+            const T inv = T(1) / mq2;
+            const T cm1 = scale * ce * inv;
+            const cplx<T> dot = mk<T>(qx * sx.x + qy * sy.x + qz0 * sz.x, qx * sx.y + qy * sy.y + qz0 * sz.y);
+            ux = mk<T>(cm1 * (sx.x - qx * inv * dot.x), cm1 * (sx.y - qx * inv * dot.y));
+            uy = mk<T>(cm1 * (sy.x - qy * inv * dot.x), cm1 * (sy.y - qy * inv * dot.y));
+            uz = mk<T>(cm1 * (sz.x - qz0 * inv * dot.x), cm1 * (sz.y - qz0 * inv * dot.y));
+          }
+          set[0][o] = ux;
+          set[1][o] = uy;
+          set[2][o] = uz;
+        }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        cplx<T>* Lc = set[c] + line * LS;
+        __syncwarp();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) v[b * RL + r] = Lc[pad(out_index<N, -1>(t, b, r))];
+        Ops::inverse_to_line(v, Lc, t, tw);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Ops::store_tile(set[c], a.u3[c] + plane_base, f0);
+    }
+  } else {  // kPencilInit(Adv): W^0 from psi^0 and N(psi^0); P^0 from psi^0
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
     Ops::forward(v, L, t, tw);
@@ -338,13 +500,51 @@ pencil_kernel(PencilArgs<T> a) {
       }
   }
 
-  if constexpr (MODE != kPencilEnergy) {
+  if constexpr (MODE == kPencilStep || MODE == kPencilInit || MODE == kPencilXMul || MODE == kPencilAdjInit ||
+                MODE == kPencilAdj || MODE == kPencilAdjOut) {
     Ops::inverse_to_line(v, L, t, tw);
     __syncthreads();
     Ops::store_tile(buf, a.dst + plane_base, f0);
+  } else if constexpr (MODE == kPencilStepAdv || MODE == kPencilInitAdv) {
+    if constexpr (!DCT) {
+      // v = scale psihat^{n+1}; emit the partials of v, i q_x v and opSH v
+      // (periodicFFT/pf3d.cpp:404-407), one inverse x transform each
+      cplx<T>* stash = buf + TK * LS + line * LS;
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) stash[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
+      __syncwarp();
+      const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha);
+      cplx<T>* outs[3] = {a.dst, a.dst_x, a.dst_sh};
+#pragma unroll 1
+      for (int o = 0; o < 3; ++o) {
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) {
+            const int kx = out_index<N, -1>(t, b, r);
+            const cplx<T> val = stash[pad(kx)];
+            const T qx = __ldg(&a.q[kx]);
+            if (o == 0) {
+              v[b * RL + r] = val;
+            } else if (o == 1) {
+              v[b * RL + r] = mk<T>(-qx * val.y, qx * val.x);
+            } else {
+              const T d = qx * qx + qy * qy + qz0 * qz0 - q02;
+              v[b * RL + r] = cscale<T>(val, alpha * d * d);
+            }
+          }
+        Ops::inverse_to_line(v, L, t, tw);
+        __syncthreads();
+        Ops::store_tile(buf, outs[o] + plane_base, f0);
+        __syncthreads();
+      }
+    }
   }
 
-  if (want_energy && MODE != kPencilInit) {
+  if (want_energy && (MODE == kPencilStep || MODE == kPencilStepAdv || MODE == kPencilEnergy)) {
     const double tot = block_sum(acc.s, scratch);
     if (threadIdx.x == 0) a.red[size_t(rep) * gridDim.x + blockIdx.x] = tot;
   }

@@ -26,7 +26,14 @@
 
 namespace shb {
 
-enum PlaneMode : int { kPlaneStep = 0, kPlaneInit = 1, kPlaneGetPsi = 2 };
+enum PlaneMode : int { kPlaneStep = 0, kPlaneInit = 1, kPlaneGetPsi = 2, kPlaneInvReal = 3, kPlaneFwdReal = 4, kPlaneAdj = 5 };
+// spectral multiplier applied to the partial spectrum as the plane is loaded
+enum SpecMult : int { kMulNone = 0, kMulIqy = 1, kMulIqz = 2, kMulNegQy2 = 3 };
+// real-space operation of kPlaneFwdReal
+enum RealOp : int {
+  kOpProduct = 0,   // in[0] * in[1]                      (stress S_i = (L psi) d_i psi)
+  kOpAdvected = 1,  // N(in[0]) + penalty - sum_i in[4+i] in[1+i]  (nonlinearity with -u.grad psi)
+};
 
 __host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -78,6 +85,13 @@ struct PlaneArgs {
   const cplx<T>* tw;      // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
   int flags;
+  // real-field modes (periodic): wavenumber table, multiplier, real inputs / output
+  const T* q;
+  int mult;
+  int op;
+  const T* real_in[7];
+  T* real_out;
+  double coef;  // adjoint: coefficient c_n of mu^{n+1}
 };
 
 // Cluster barrier.  RELEASE orders this thread's earlier shared-memory writes
@@ -195,7 +209,21 @@ struct PlaneOps {
   static constexpr int THREADS = Cfg::THREADS;
 
   // ---- column phase, inverse direction ---------------------------------
-  static __device__ void col_load(cplx<T>* buf, const cplx<T>* __restrict__ plane, int rank) {
+  // multiply a periodic spectral value at (ky, kz) by i q_y, i q_z or -q_y^2
+  static __device__ __forceinline__ cplx<T> apply_mult(cplx<T> v, int mult, const T* q, int ky, int kz) {
+    if (mult == kMulIqy || mult == kMulIqz) {
+      const T qq = __ldg(&q[mult == kMulIqy ? ky : kz]);
+      return mk<T>(-qq * v.y, qq * v.x);
+    }
+    if (mult == kMulNegQy2) {
+      const T qq = __ldg(&q[ky]);
+      return cscale<T>(v, -qq * qq);
+    }
+    return v;
+  }
+
+  static __device__ void col_load(cplx<T>* buf, const cplx<T>* __restrict__ plane, int rank, int mult = kMulNone,
+                                  const T* q = nullptr) {
     const int c0 = rank * NC;
     // NC * N == THREADS * E: every thread issues its E loads before any store
     cplx<T> tmp[E];
@@ -204,6 +232,13 @@ struct PlaneOps {
       const int idx = threadIdx.x + THREADS * e;
       tmp[e] = plane[(idx / NC) * (N / 2) + c0 + idx % NC];
     }
+    if (mult != kMulNone) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + THREADS * e;
+        tmp[e] = apply_mult(tmp[e], mult, q, idx / NC, c0 + idx % NC);
+      }
+    }
     constexpr int KPT = (N + THREADS - 1) / THREADS;  // ky per thread for the kz=0 / N/2 columns
     cplx<T> nyq[KPT];
     if constexpr (!DCT) {
@@ -211,7 +246,7 @@ struct PlaneOps {
 #pragma unroll
         for (int m = 0; m < KPT; ++m) {
           const int ky = threadIdx.x + m * THREADS;
-          if (ky < N) nyq[m] = plane[N * (N / 2) + ky];
+          if (ky < N) nyq[m] = apply_mult(plane[N * (N / 2) + ky], mult, q, ky, N / 2);
         }
       }
     }
@@ -617,8 +652,12 @@ plane_kernel(PlaneArgs<T> a) {
   const int y0 = rank * ROWS + 2 * line;
   cplx<T> v[E];
 
-  if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi) {
-    Ops::col_load(buf, a.src + plane_off, rank);
+  if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi || MODE == kPlaneInvReal || MODE == kPlaneAdj) {
+    if constexpr (MODE == kPlaneInvReal) {
+      Ops::col_load(buf, a.src + plane_off, rank, a.mult, a.q);
+    } else {
+      Ops::col_load(buf, a.src + plane_off, rank);
+    }
     Ops::col_inverse_to_rows(buf, xs, rank, tw);
     Ops::row_inverse(v, buf, xs, L, line, t, tw);
 
@@ -657,11 +696,74 @@ plane_kernel(PlaneArgs<T> a) {
         }
       }
     }
+    if (MODE == kPlaneInvReal || MODE == kPlaneAdj || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const size_t ia = real_off + size_t(y0) * N + Ops::row_z(t, b, r);
+          a.real_out[ia] = v[b * RL + r].x;
+          a.real_out[ia + N] = v[b * RL + r].y;
+        }
+    }
+    if constexpr (MODE == kPlaneAdj) {
+      // g^n = N'(psi^n) (c_n mu^{n+1} - mu^{n+2});  v holds mu^{n+1}
+      const T beta = T(a.pp.beta), gamma = T(a.pp.gamma), c = T(a.coef);
+      const T* psi = a.real_in[1];
+      const T* mu2 = a.real_in[0];
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const size_t ia = real_off + size_t(y0) * N + Ops::row_z(t, b, r);
+          const cplx<T> m = v[b * RL + r];
+          const T ma = mu2 ? mu2[ia] : T(0), mb = mu2 ? mu2[ia + N] : T(0);
+          v[b * RL + r] = mk<T>(nonlin_deriv<T>(psi[ia], beta, gamma, a.pp.nonlin) * (c * m.x - ma),
+                                nonlin_deriv<T>(psi[ia + N], beta, gamma, a.pp.nonlin) * (c * m.y - mb));
+        }
+      Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
+      Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
+    }
     if constexpr (MODE == kPlaneStep) {
       row_nonlin<T, N, CL, DCT>(v, L, t, a.pp);
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
     }
+  } else if constexpr (MODE == kPlaneFwdReal) {
+    // real fields -> pointwise op -> partial spectrum
+    constexpr int R0 = radix_of<N, -1, 0>();
+    const T beta = T(a.pp.beta), gamma = T(a.pp.gamma);
+    const T cpen = T(2.0 * a.pp.w_mid * a.pp.inv_dz2);
+#pragma unroll
+    for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int n = in_index<N, -1>(t, b, r);
+        const int z = DCT ? mk_perm<N>(n) : n;
+        const size_t ia = real_off + size_t(y0) * N + z, ib = ia + N;
+        T oa, ob;
+        if (a.op == kOpProduct) {
+          oa = a.real_in[0][ia] * a.real_in[1][ia];
+          ob = a.real_in[0][ib] * a.real_in[1][ib];
+        } else {
+          const T* ps = a.real_in[0];
+          const T pa = ps[ia], pb = ps[ib];
+          oa = nonlin_eval<T>(pa, beta, gamma, a.pp.nonlin);
+          ob = nonlin_eval<T>(pb, beta, gamma, a.pp.nonlin);
+          if (a.pp.w_mid != 0.0 && z == N / 2) {
+            oa += cpen * (ps[ia - 1] - T(2) * pa + ps[ia + 1]);
+            ob += cpen * (ps[ib - 1] - T(2) * pb + ps[ib + 1]);
+          }
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            oa -= a.real_in[4 + c][ia] * a.real_in[1 + c][ia];
+            ob -= a.real_in[4 + c][ib] * a.real_in[1 + c][ib];
+          }
+        }
+        v[b * R0 + r] = mk<T>(oa, ob);
+      }
+    Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
+    Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
   } else {  // kPlaneInit: real psi -> partial spectra of psi (dst2) and N(psi) (dst)
     const double* src = a.psi_in + real_off;
     for (int field = 0; field < 2; ++field) {

@@ -42,6 +42,32 @@ __global__ void finalize_kernel(const double* red_plane, int nbp, const double* 
   }
 }
 
+__global__ void adj_accumulate_kernel(const double* red, int nblocks, double* acc) {
+  __shared__ double scratch[32];
+  const int rep = blockIdx.x;
+  KahanSum s0, s1;
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    s0.add(red[(size_t(rep) * nblocks + b) * 2 + 0]);
+    s1.add(red[(size_t(rep) * nblocks + b) * 2 + 1]);
+  }
+  const double te = block_sum(s0.s, scratch);
+  const double tq = block_sum(s1.s, scratch);
+  if (threadIdx.x == 0) {
+    double* a = acc + size_t(rep) * 4;
+    KahanSum k;
+    k.s = a[0];
+    k.c = a[1];
+    k.add(te);
+    a[0] = k.s;
+    a[1] = k.c;
+    k.s = a[2];
+    k.c = a[3];
+    k.add(tq);
+    a[2] = k.s;
+    a[3] = k.c;
+  }
+}
+
 }  // namespace shb
 
 #define API_CUDA(h, expr)                                                        \
@@ -134,7 +160,6 @@ int sh_create(const sh_params* p, sh_handle** out) {
   if (p->l1_interval < 0) return fail(nullptr, SH_EINVAL, "l1_interval must be >= 0");
   if (p->advection && p->boundary != SH_PERIODIC)
     return fail(nullptr, SH_EINVAL, "advection is defined for the periodic boundary only");
-  if (p->advection) return fail(nullptr, SH_EUNSUPPORTED, "advection is not built into this library version");
   if (p->sub_sigma != 0.0) return fail(nullptr, SH_EUNSUPPORTED, "substrate penalty is not built into this library version");
   if (p->variant < 0) return fail(nullptr, SH_EINVAL, "variant must be >= 0");
 
@@ -321,8 +346,18 @@ int sh_l1(sh_handle* h, double* out, int* count) {
   return SH_OK;
 }
 
-int sh_surface_step(sh_handle* h, int*, double*, double*, double*) {
-  return fail(h, SH_EUNSUPPORTED, "surface tracking is not built into this library version");
+int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kgauss) {
+  if (!h || !h->s || !z || !vn || !hmean || !kgauss) return fail(h, SH_EINVAL, "null argument");
+  if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
+  return h->s->surface_step(z, vn, hmean, kgauss);
+}
+
+int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every, double* g_eps,
+               double* g_q0, double* g_psi0) {
+  if (!h || !h->s || !psi0 || !dl_dpsi_t || !g_eps || !g_q0 || !g_psi0) return fail(h, SH_EINVAL, "null argument");
+  int rc = h->s->adjoint(psi0, nsteps, dl_dpsi_t, ckpt_every, g_eps, g_q0, g_psi0);
+  if (rc == SH_OK) h->s->ready = true;
+  return rc;
 }
 
 int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes) {

@@ -10,7 +10,13 @@ namespace cg = cooperative_groups;
 
 enum NonlinKind : int { kQuintic = 0, kQuadCubic = 1 };
 enum SchemeKind : int { kCNAB2 = 0, kIMEXEuler = 1 };
-enum PassFlags : int { kFlPsiOut = 1, kFlL1 = 2, kFlEnergy = 4 };
+enum PassFlags : int {
+  kFlPsiOut = 1,    // plane: write psi (double)
+  kFlL1 = 2,        // plane: L1 monitor partial sums
+  kFlEnergy = 4,    // plane / pencil: energy partial sums
+  kFlRealOut = 8,   // plane step: write psi (T) to real_out
+  kFlSpecOut = 16,  // pencil step: write psihat^{n+1} (pencil-major) to spec_out
+};
 
 // Per-launch scalar parameters of the pointwise stages.
 struct PointParams {
@@ -32,6 +38,14 @@ __device__ __forceinline__ T nonlin_eval(T p, T beta, T gamma, int kind) {
   if (kind == kQuintic) return p * p2 * (beta - gamma * p2);
   // beta psi^2 - gamma psi^3
   return p2 * (beta - gamma * p);
+}
+
+// dN/dpsi
+template <typename T>
+__device__ __forceinline__ T nonlin_deriv(T p, T beta, T gamma, int kind) {
+  const T p2 = p * p;
+  if (kind == kQuintic) return p2 * (T(3) * beta - T(5) * gamma * p2);
+  return p * (T(2) * beta - T(3) * gamma * p);
 }
 
 // Local part of the Lyapunov density (energyPsi.m:225-228 without the gradient

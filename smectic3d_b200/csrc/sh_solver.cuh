@@ -9,6 +9,7 @@
 #include "../../include/smectic_b200.h"
 #include "pencil_kernel.cuh"
 #include "plane_kernel.cuh"
+#include "surface_kernel.cuh"
 
 namespace shb {
 
@@ -25,6 +26,10 @@ namespace shb {
 // what = 0: energy dv (local + alpha/2 norm spec); what = 1: L1 = A / (dt B)
 __global__ void finalize_kernel(const double* red_plane, int nbp, const double* red_spec, int nbs, int what,
                                 double dv, double spec_norm, double alpha, double dt, double* out);
+// Adds the per-CTA (eps, q0) gradient partials of one adjoint step to the
+// running per-replica totals acc[rep][4] = {sum_eps, comp_eps, sum_q0, comp_q0}
+// (Kahan-compensated across steps).
+__global__ void adj_accumulate_kernel(const double* red, int nblocks, double* acc);
 
 struct SolverBase {
   sh_params p{};
@@ -60,6 +65,7 @@ struct SolverBase {
     cudaFree(d_trace);
     for (auto& e : prof_ev)
       if (e) cudaEventDestroy(e);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (stream) cudaStreamDestroy(stream);
   }
   size_t n3() const { return size_t(p.n) * p.n * p.n; }
@@ -69,11 +75,19 @@ struct SolverBase {
   // per-launch event timing of the two passes (nullptr: off)
   double* prof_ms = nullptr;
   cudaEvent_t prof_ev[3] = {nullptr, nullptr, nullptr};
+  // CUDA graph of kGraphChunk plain steps (replayed when no per-step host
+  // bookkeeping is needed: no energy trace, L1 monitor, profiling or history)
+  static constexpr int kGraphChunk = 16;
+  cudaGraphExec_t graph_exec = nullptr;
+  bool use_graphs = true;
   virtual int psi_to_dpsi() = 0;       // current psi -> d_psi
   virtual int energy_now(double* host) = 0;
   virtual size_t state_bytes() const = 0;
   virtual int save_state(void* host) = 0;
   virtual int load_state(const void* host) = 0;
+  virtual int surface_step(int* z, double* vn, double* hh, double* kk) = 0;
+  virtual int adjoint(const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every, double* g_eps,
+                      double* g_q0, double* g_psi0) = 0;
 };
 
 template <typename T, int N, int CL, bool DCT>
@@ -86,6 +100,21 @@ struct Solver final : SolverBase {
   cplx<T>* P = nullptr;
   cplx<T>* Nt = nullptr;
   cplx<T>* tw = nullptr;  // [forward | inverse | quarter-wave] twiddle table
+  // Stokes advection (periodic): partials of i q_x psihat and opSH psihat, the
+  // three stress / velocity partials, and the real fields
+  // psi, d_x psi, d_y psi, d_z psi, L psi (then u_x), u_y, u_z
+  cplx<T>* Px = nullptr;
+  cplx<T>* PSH = nullptr;
+  cplx<T>* S3[3] = {nullptr, nullptr, nullptr};
+  T* R[8] = {};      // psi, d_x psi, d_y psi, d_z psi, L psi, u_x, u_y, u_z of the current state
+  T* SR[4] = {};     // surface pass: psi_xx, psi_yy, psi_xy, H-numerator (allocated on first use)
+  int* d_zout = nullptr;
+  double* d_surf[3] = {nullptr, nullptr, nullptr};
+  bool real_fields_current = false;
+  // adjoint: per-step history of a recomputed segment (psihat pencil-major, psi real)
+  cplx<T>* hist_spec = nullptr;
+  T* hist_real = nullptr;
+  int hist_pos = 0;
   T* q = nullptr;
 
   ~Solver() override {
@@ -95,6 +124,13 @@ struct Solver final : SolverBase {
     cudaFree(Nt);
     cudaFree(tw);
     cudaFree(q);
+    cudaFree(Px);
+    cudaFree(PSH);
+    for (auto* p3 : S3) cudaFree(p3);
+    for (auto* r : R) cudaFree(r);
+    for (auto* r : SR) cudaFree(r);
+    cudaFree(d_zout);
+    for (auto* d : d_surf) cudaFree(d);
   }
 
   size_t field_elems() const { return size_t(p.batch) * N * FP; }
@@ -133,6 +169,17 @@ struct Solver final : SolverBase {
     SHB_CUDA(cudaMalloc(&W, fe * sizeof(cplx<T>)));
     SHB_CUDA(cudaMalloc(&P, fe * sizeof(cplx<T>)));
     SHB_CUDA(cudaMalloc(&Nt, fe * sizeof(cplx<T>)));
+    if (p.advection) {
+      if constexpr (DCT) {
+        err = "advection is defined for the periodic boundary only";
+        return SH_EINVAL;
+      } else {
+        SHB_CUDA(cudaMalloc(&Px, fe * sizeof(cplx<T>)));
+        SHB_CUDA(cudaMalloc(&PSH, fe * sizeof(cplx<T>)));
+        for (auto& p3 : S3) SHB_CUDA(cudaMalloc(&p3, fe * sizeof(cplx<T>)));
+        for (auto& r : R) SHB_CUDA(cudaMalloc(&r, size_t(p.batch) * N * N * N * sizeof(T)));
+      }
+    }
     SHB_CUDA(cudaMalloc(&tw, tw_total<N>() * sizeof(cplx<T>)));
     SHB_CUDA(cudaMalloc(&q, N * sizeof(T)));
     SHB_CUDA(cudaMalloc(&d_red_plane, size_t(p.batch) * N * CL * 3 * sizeof(double)));
@@ -154,9 +201,20 @@ struct Solver final : SolverBase {
     if ((rc = set_attrs(plane_fn<kPlaneStep>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneInit>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneGetPsi>(), PC::SMEM, true))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilStep>(), QC::SMEM, false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilInit>(), QC::SMEM, false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilEnergy>(), QC::SMEM, false))) return rc;
+    if ((rc = set_attrs(plane_fn<kPlaneInvReal>(), PC::SMEM, true))) return rc;
+    if ((rc = set_attrs(plane_fn<kPlaneFwdReal>(), PC::SMEM, true))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilStep>(), QC::smem(kPencilStep), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilInit>(), QC::smem(kPencilInit), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilEnergy>(), QC::smem(kPencilEnergy), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilStepAdv>(), QC::smem(kPencilStepAdv), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilInitAdv>(), QC::smem(kPencilInitAdv), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilStokes>(), QC::smem(kPencilStokes), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilXMul>(), QC::smem(kPencilXMul), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilSpec>(), QC::smem(kPencilSpec), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilAdjInit>(), QC::smem(kPencilAdjInit), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilAdj>(), QC::smem(kPencilAdj), false))) return rc;
+    if ((rc = set_attrs(pencil_fn<kPencilAdjOut>(), QC::smem(kPencilAdjOut), false))) return rc;
+    if ((rc = set_attrs(plane_fn<kPlaneAdj>(), PC::SMEM, true))) return rc;
     return SH_OK;
   }
 
@@ -181,7 +239,7 @@ struct Solver final : SolverBase {
 
   template <int MODE>
   int launch_pencil(const PencilArgs<T>& a) {
-    pencil_fn<MODE>()<<<dim3(QC::TILES, p.batch, 1), QC::THREADS, QC::SMEM, stream>>>(a);
+    pencil_fn<MODE>()<<<dim3(QC::TILES, p.batch, 1), QC::THREADS, QC::smem(MODE), stream>>>(a);
     SHB_CUDA(cudaGetLastError());
     ++launches;
     return SH_OK;
@@ -193,6 +251,7 @@ struct Solver final : SolverBase {
     a.pp = point_params();
     a.red = d_red_plane;
     a.timeout = d_flag + 1;
+    a.q = q;
     return a;
   }
   PencilArgs<T> pencil_args() const {
@@ -227,7 +286,15 @@ struct Solver final : SolverBase {
     b.src2 = Nt;
     b.w = W;
     b.dst = P;
-    if ((rc = launch_pencil<kPencilInit>(b))) return rc;
+    if (p.advection) {
+      b.dst_x = Px;
+      b.dst_sh = PSH;
+      if ((rc = launch_pencil<kPencilInitAdv>(b))) return rc;
+      // the first advected N (N-hat^{-1} above discards advection, pf3d.cpp:363-374)
+      if ((rc = adv_nonlinear(0))) return rc;
+    } else {
+      if ((rc = launch_pencil<kPencilInit>(b))) return rc;
+    }
     if (p.l1_interval > 0)
       SHB_CUDA(cudaMemcpyAsync(d_stash, d_psi, size_t(p.batch) * n3() * sizeof(double), cudaMemcpyDeviceToDevice,
                                stream));
@@ -240,6 +307,38 @@ struct Solver final : SolverBase {
   }
 
   int step_async(int n) override {
+    if (use_graphs && !prof_ms && !hist_spec && !p.energy_trace && p.l1_interval == 0 && n >= kGraphChunk) {
+      int rc;
+      if (!graph_exec) {
+        // capture kGraphChunk steps once; the steps counter is restored after
+        cudaGraph_t g;
+        const long long s0 = steps, l0 = launches;
+        SHB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        rc = step_direct(kGraphChunk);
+        cudaError_t e = cudaStreamEndCapture(stream, &g);
+        steps = s0;
+        hist_pos -= kGraphChunk;
+        graph_launches = launches - l0;
+        launches = l0;
+        if (rc) return rc;
+        SHB_CUDA(e);
+        e = cudaGraphInstantiate(&graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        SHB_CUDA(e);
+      }
+      const int chunks = n / kGraphChunk;
+      for (int c = 0; c < chunks; ++c) {
+        SHB_CUDA(cudaGraphLaunch(graph_exec, stream));
+        steps += kGraphChunk;
+        launches += graph_launches;
+      }
+      return step_direct(n - chunks * kGraphChunk);
+    }
+    return step_direct(n);
+  }
+  long long graph_launches = 0;
+
+  int step_direct(int n) {
     int rc;
     const bool trace = p.energy_trace != 0;
     if (trace && n > trace_cap) {
@@ -258,16 +357,33 @@ struct Solver final : SolverBase {
       b.w = W;
       b.dst = P;
       b.flags = trace ? kFlEnergy : 0;
+      if (hist_spec) {  // adjoint recompute: keep psihat^{n+1}
+        b.flags |= kFlSpecOut;
+        b.spec_out = hist_spec + size_t(hist_pos + 1) * field_elems();
+      }
       if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[0], stream));
-      if ((rc = launch_pencil<kPencilStep>(b))) return rc;
-      if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
-      PlaneArgs<T> a = plane_args();
-      a.src = P;
-      a.dst = Nt;
-      a.flags = (trace ? kFlEnergy : 0) | (l1_now ? kFlL1 : 0) | (stash_now ? kFlPsiOut : 0);
-      a.psi_old = d_stash;
-      a.psi_out = d_stash;
-      if ((rc = launch_plane<kPlaneStep>(a))) return rc;
+      const int diag = (trace ? kFlEnergy : 0) | (l1_now ? kFlL1 : 0) | (stash_now ? kFlPsiOut : 0);
+      if (p.advection) {
+        b.dst_x = Px;
+        b.dst_sh = PSH;
+        if ((rc = launch_pencil<kPencilStepAdv>(b))) return rc;
+        if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
+        if ((rc = adv_nonlinear(diag))) return rc;
+      } else {
+        if ((rc = launch_pencil<kPencilStep>(b))) return rc;
+        if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
+        PlaneArgs<T> a = plane_args();
+        a.src = P;
+        a.dst = Nt;
+        a.flags = diag;
+        a.psi_old = d_stash;
+        a.psi_out = d_stash;
+        if (hist_real) {  // adjoint recompute: keep psi^{n+1}
+          a.flags |= kFlRealOut;
+          a.real_out = hist_real + size_t(hist_pos + 1) * size_t(p.batch) * N * N * N;
+        }
+        if ((rc = launch_plane<kPlaneStep>(a))) return rc;
+      }
       if (prof_ms) {
         float t0, t1;
         SHB_CUDA(cudaEventRecord(prof_ev[2], stream));
@@ -283,8 +399,63 @@ struct Solver final : SolverBase {
         ++l1_count;
       }
       ++steps;
+      ++hist_pos;
     }
     return SH_OK;
+  }
+
+  // Nonlinear term with Stokes advection of the state held in P, Px, PSH
+  // (periodicFFT/pf3d.cpp:397-465): psi, grad psi and L psi in real space,
+  // stress S = (L psi) grad psi, Stokes velocity u, then
+  // N = beta psi^3 - gamma psi^5 (+ penalty) - u.grad psi, forward y,z -> Nt.
+  int adv_nonlinear(int diag) {
+    if constexpr (DCT) {
+      return SH_EINVAL;
+    } else {
+      int rc;
+      const cplx<T>* src[5] = {P, Px, P, P, PSH};
+      const int mult[5] = {kMulNone, kMulNone, kMulIqy, kMulIqz, kMulNone};
+      for (int i = 0; i < 5; ++i) {
+        PlaneArgs<T> a = plane_args();
+        a.src = src[i];
+        a.mult = mult[i];
+        a.real_out = R[i];
+        if (i == 0) {
+          a.flags = diag;
+          a.psi_old = d_stash;
+          a.psi_out = d_stash;
+        }
+        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      }
+      for (int c = 0; c < 3; ++c) {
+        PlaneArgs<T> a = plane_args();
+        a.op = kOpProduct;
+        a.real_in[0] = R[4];
+        a.real_in[1] = R[1 + c];
+        a.dst = S3[c];
+        if ((rc = launch_plane<kPlaneFwdReal>(a))) return rc;
+      }
+      PencilArgs<T> b = pencil_args();
+      for (int c = 0; c < 3; ++c) {
+        b.s3[c] = S3[c];
+        b.u3[c] = S3[c];
+      }
+      if ((rc = launch_pencil<kPencilStokes>(b))) return rc;
+      for (int c = 0; c < 3; ++c) {
+        PlaneArgs<T> a = plane_args();
+        a.src = S3[c];
+        a.real_out = R[5 + c];
+        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      }
+      PlaneArgs<T> a = plane_args();
+      a.op = kOpAdvected;
+      for (int i = 0; i < 4; ++i) a.real_in[i] = R[i];
+      for (int c = 0; c < 3; ++c) a.real_in[4 + c] = R[5 + c];
+      a.dst = Nt;
+      if ((rc = launch_plane<kPlaneFwdReal>(a))) return rc;
+      real_fields_current = true;
+      return SH_OK;
+    }
   }
 
   int psi_to_dpsi() override {
@@ -314,13 +485,17 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
-  size_t state_bytes() const override { return 3 * field_elems() * sizeof(cplx<T>); }
+  size_t state_bytes() const override { return (p.advection ? 5 : 3) * field_elems() * sizeof(cplx<T>); }
   int save_state(void* host) override {
     const size_t fb = field_elems() * sizeof(cplx<T>);
     char* h = static_cast<char*>(host);
     SHB_CUDA(cudaMemcpyAsync(h, W, fb, cudaMemcpyDeviceToHost, stream));
     SHB_CUDA(cudaMemcpyAsync(h + fb, P, fb, cudaMemcpyDeviceToHost, stream));
     SHB_CUDA(cudaMemcpyAsync(h + 2 * fb, Nt, fb, cudaMemcpyDeviceToHost, stream));
+    if (p.advection) {
+      SHB_CUDA(cudaMemcpyAsync(h + 3 * fb, Px, fb, cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(h + 4 * fb, PSH, fb, cudaMemcpyDeviceToHost, stream));
+    }
     SHB_CUDA(cudaStreamSynchronize(stream));
     return SH_OK;
   }
@@ -330,10 +505,257 @@ struct Solver final : SolverBase {
     SHB_CUDA(cudaMemcpyAsync(W, h, fb, cudaMemcpyHostToDevice, stream));
     SHB_CUDA(cudaMemcpyAsync(P, h + fb, fb, cudaMemcpyHostToDevice, stream));
     SHB_CUDA(cudaMemcpyAsync(Nt, h + 2 * fb, fb, cudaMemcpyHostToDevice, stream));
+    if (p.advection) {
+      SHB_CUDA(cudaMemcpyAsync(Px, h + 3 * fb, fb, cudaMemcpyHostToDevice, stream));
+      SHB_CUDA(cudaMemcpyAsync(PSH, h + 4 * fb, fb, cudaMemcpyHostToDevice, stream));
+    }
     SHB_CUDA(cudaStreamSynchronize(stream));
     ready = true;
     psi0_valid = false;
+    real_fields_current = false;
     return SH_OK;
+  }
+
+  // Discrete adjoint of the plain periodic CNAB2 loop (reverse sweep
+  // lambda^n = A lambda^{n+1} + N'(psi^n)(c_n B lambda^{n+1} - B lambda^{n+2}),
+  // c_n = 3, c_0 = 2) for a loss whose gradient with respect to psi^T is
+  // dl_dpsi_t.  The forward states are checkpointed every ckpt_every steps and
+  // recomputed segment by segment; the (eps, q0) gradients accumulate in FP64.
+  int adjoint(const double* psi0, int nsteps, const double* dl_dpsi_t, int K, double* g_eps, double* g_q0,
+              double* g_psi0) override {
+    if constexpr (DCT) {
+      err = "the adjoint is built for the periodic boundary";
+      return SH_EUNSUPPORTED;
+    } else {
+      if (p.advection || p.scheme != kCNAB2 || p.w_mid != 0.0) {
+        err = "the adjoint covers the plain CNAB2 step without advection or penalty";
+        return SH_EUNSUPPORTED;
+      }
+      if (nsteps < 1 || K < 1) {
+        err = "nsteps and ckpt_every must be >= 1";
+        return SH_EINVAL;
+      }
+      int rc;
+      const size_t fe = field_elems();
+      const size_t nr = size_t(p.batch) * N * N * N;
+      const int nseg = (nsteps + K - 1) / K;
+      const bool saved_trace = p.energy_trace != 0;
+      const int saved_l1 = p.l1_interval;
+      p.energy_trace = 0;
+      p.l1_interval = 0;
+      struct Bufs {
+        cplx<T>* ck = nullptr;   // nseg states x {W, P, Nt}
+        cplx<T>* hs = nullptr;   // (K+1) psihat
+        T* hr = nullptr;         // (K+1) psi
+        cplx<T>* lam = nullptr;  // lambdahat, pencil-major
+        cplx<T>* gp = nullptr;   // partial of g
+        cplx<T>* mp = nullptr;   // partial of mu
+        T* mu[2] = {nullptr, nullptr};
+        double* red = nullptr;
+        double* acc = nullptr;
+        ~Bufs() {
+          cudaFree(ck); cudaFree(hs); cudaFree(hr); cudaFree(lam); cudaFree(gp); cudaFree(mp);
+          cudaFree(mu[0]); cudaFree(mu[1]); cudaFree(red); cudaFree(acc);
+        }
+      } bf;
+      auto restore = [&]() { p.energy_trace = saved_trace; p.l1_interval = saved_l1; hist_spec = nullptr; hist_real = nullptr; };
+#define ADJ_CUDA(expr)                                                           \
+  do {                                                                           \
+    cudaError_t e_ = (expr);                                                     \
+    if (e_ != cudaSuccess) {                                                     \
+      err = std::string(#expr) + ": " + cudaGetErrorString(e_);                  \
+      restore();                                                                 \
+      return e_ == cudaErrorMemoryAllocation ? SH_ENOMEM : SH_ECUDA;             \
+    }                                                                            \
+  } while (0)
+#define ADJ_RC(expr)       \
+  do {                     \
+    if ((rc = (expr))) {   \
+      restore();           \
+      return rc;           \
+    }                      \
+  } while (0)
+      ADJ_CUDA(cudaMalloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
+      ADJ_CUDA(cudaMalloc(&bf.hs, size_t(K + 1) * fe * sizeof(cplx<T>)));
+      ADJ_CUDA(cudaMalloc(&bf.hr, size_t(K + 1) * nr * sizeof(T)));
+      ADJ_CUDA(cudaMalloc(&bf.lam, fe * sizeof(cplx<T>)));
+      ADJ_CUDA(cudaMalloc(&bf.gp, fe * sizeof(cplx<T>)));
+      ADJ_CUDA(cudaMalloc(&bf.mp, fe * sizeof(cplx<T>)));
+      ADJ_CUDA(cudaMalloc(&bf.mu[0], nr * sizeof(T)));
+      ADJ_CUDA(cudaMalloc(&bf.mu[1], nr * sizeof(T)));
+      ADJ_CUDA(cudaMalloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
+      ADJ_CUDA(cudaMalloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
+      ADJ_CUDA(cudaMemsetAsync(bf.acc, 0, size_t(p.batch) * 4 * sizeof(double), stream));
+      const size_t fb = fe * sizeof(cplx<T>);
+      // ---- forward sweep with checkpoints at s = 0, K, 2K, ...
+      ADJ_CUDA(cudaMemcpyAsync(d_psi, psi0, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
+      ADJ_RC(init_from_psi());
+      for (int sg = 0; sg < nseg; ++sg) {
+        cplx<T>* c = bf.ck + size_t(sg) * 3 * fe;
+        ADJ_CUDA(cudaMemcpyAsync(c, W, fb, cudaMemcpyDeviceToDevice, stream));
+        ADJ_CUDA(cudaMemcpyAsync(c + fe, P, fb, cudaMemcpyDeviceToDevice, stream));
+        ADJ_CUDA(cudaMemcpyAsync(c + 2 * fe, Nt, fb, cudaMemcpyDeviceToDevice, stream));
+        const int s1 = (sg + 1) * K < nsteps ? (sg + 1) * K : nsteps;
+        ADJ_RC(step_async(s1 - sg * K));
+      }
+      // ---- lambda^T -> lambdahat^T and the partial of mu^T = B lambda^T
+      ADJ_CUDA(cudaMemcpyAsync(d_psi, dl_dpsi_t, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
+      {
+        PlaneArgs<T> a = plane_args();
+        a.psi_in = d_psi;
+        a.dst2 = bf.gp;   // partial of lambda^T
+        a.dst = bf.mp;    // (the N of lambda^T, unused scratch)
+        ADJ_RC(launch_plane<kPlaneInit>(a));
+        PencilArgs<T> b = pencil_args();
+        b.src = bf.gp;
+        b.w = bf.lam;
+        b.dst = bf.mp;
+        ADJ_RC(launch_pencil<kPencilAdjInit>(b));
+      }
+      int cur = 0;          // mu buffer receiving mu^{n+1}; the other holds mu^{n+2}
+      bool have_mu2 = false;
+      // ---- reverse sweep, one recomputed segment at a time
+      for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int s0 = sg * K;
+        const int s1 = (sg + 1) * K < nsteps ? (sg + 1) * K : nsteps;
+        const cplx<T>* c = bf.ck + size_t(sg) * 3 * fe;
+        ADJ_CUDA(cudaMemcpyAsync(W, c, fb, cudaMemcpyDeviceToDevice, stream));
+        ADJ_CUDA(cudaMemcpyAsync(P, c + fe, fb, cudaMemcpyDeviceToDevice, stream));
+        ADJ_CUDA(cudaMemcpyAsync(Nt, c + 2 * fe, fb, cudaMemcpyDeviceToDevice, stream));
+        {  // psihat^{s0} and psi^{s0} of the segment's first state
+          PencilArgs<T> b = pencil_args();
+          b.src = P;
+          b.spec_out = bf.hs;
+          ADJ_RC(launch_pencil<kPencilSpec>(b));
+          PlaneArgs<T> a = plane_args();
+          a.src = P;
+          a.real_out = bf.hr;
+          ADJ_RC(launch_plane<kPlaneInvReal>(a));
+        }
+        hist_spec = bf.hs;
+        hist_real = bf.hr;
+        hist_pos = 0;
+        ADJ_RC(step_async(s1 - s0));
+        hist_spec = nullptr;
+        hist_real = nullptr;
+        for (int n = s1 - 1; n >= s0; --n) {
+          const int j = n - s0;
+          PlaneArgs<T> a = plane_args();
+          a.src = bf.mp;                       // partial of mu^{n+1}
+          a.real_out = bf.mu[cur];             // mu^{n+1}
+          a.real_in[0] = have_mu2 ? bf.mu[cur ^ 1] : nullptr;  // mu^{n+2}
+          a.real_in[1] = bf.hr + size_t(j) * nr;               // psi^n
+          a.coef = n >= 1 ? 3.0 : 2.0;
+          a.dst = bf.gp;                       // partial of g^n
+          ADJ_RC(launch_plane<kPlaneAdj>(a));
+          PencilArgs<T> b = pencil_args();
+          b.src = bf.gp;
+          b.w = bf.lam;                        // lambdahat^{n+1} -> lambdahat^n
+          b.spec_a = bf.hs + size_t(j) * fe;   // psihat^n
+          b.spec_b = bf.hs + size_t(j + 1) * fe;
+          b.dst = bf.mp;                       // partial of mu^n
+          b.red = bf.red;
+          ADJ_RC(launch_pencil<kPencilAdj>(b));
+          adj_accumulate_kernel<<<p.batch, 256, 0, stream>>>(bf.red, QC::TILES, bf.acc);
+          ADJ_CUDA(cudaGetLastError());
+          launches += 1;
+          cur ^= 1;
+          have_mu2 = true;
+        }
+      }
+      // ---- lambda^0 = dL/dpsi^0 in real space
+      {
+        PencilArgs<T> b = pencil_args();
+        b.w = bf.lam;
+        b.dst = bf.gp;
+        ADJ_RC(launch_pencil<kPencilAdjOut>(b));
+        PlaneArgs<T> a = plane_args();
+        a.src = bf.gp;
+        a.psi_out = d_psi;
+        a.flags = kFlPsiOut;
+        ADJ_RC(launch_plane<kPlaneGetPsi>(a));
+      }
+      std::vector<double> acc(size_t(p.batch) * 4);
+      ADJ_CUDA(cudaMemcpyAsync(acc.data(), bf.acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      ADJ_CUDA(cudaMemcpyAsync(g_psi0, d_psi, nr * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      ADJ_CUDA(cudaStreamSynchronize(stream));
+      for (int r = 0; r < p.batch; ++r) {
+        g_eps[r] = acc[size_t(r) * 4 + 0];
+        g_q0[r] = acc[size_t(r) * 4 + 2];
+      }
+      psi0_valid = false;
+      restore();
+#undef ADJ_CUDA
+#undef ADJ_RC
+      return SH_OK;
+    }
+  }
+
+  // surfTrack pass (periodicFFT/surfTrack.cpp:592-626, 744-806): one advected
+  // step; the crossing of psi^{n+1} per (x, y) column with v_n, H, K from the
+  // fields of state n.
+  int surface_step(int* z, double* vn, double* hh, double* kk) override {
+    if constexpr (DCT) {
+      err = "surface tracking is defined for the periodic boundary";
+      return SH_EINVAL;
+    } else {
+      if (!p.advection) {
+        err = "surface tracking runs the advected step (advection = 1)";
+        return SH_EINVAL;
+      }
+      int rc;
+      const size_t nr = size_t(p.batch) * N * N * N, nc = size_t(p.batch) * N * N;
+      if (!SR[0]) {
+        for (auto& r : SR) SHB_CUDA(cudaMalloc(&r, nr * sizeof(T)));
+        SHB_CUDA(cudaMalloc(&d_zout, nc * sizeof(int)));
+        for (auto& d : d_surf) SHB_CUDA(cudaMalloc(&d, nc * sizeof(double)));
+      }
+      if (!real_fields_current && (rc = adv_nonlinear(0))) return rc;
+      // second derivatives of psi^n: psi_xx = C2R(-q_x^2 psihat), psi_yy, psi_xy
+      PencilArgs<T> b = pencil_args();
+      b.src = Px;
+      b.dst = S3[0];
+      if ((rc = launch_pencil<kPencilXMul>(b))) return rc;
+      const cplx<T>* src[3] = {S3[0], P, Px};
+      const int mult[3] = {kMulNone, kMulNegQy2, kMulIqy};
+      for (int i = 0; i < 3; ++i) {
+        PlaneArgs<T> a = plane_args();
+        a.src = src[i];
+        a.mult = mult[i];
+        a.real_out = SR[i];
+        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      }
+      SurfArgs<T> sa;
+      sa.psi = R[0];
+      sa.gx = R[1];
+      sa.gy = R[2];
+      sa.gz = R[3];
+      sa.lpsi = R[4];
+      sa.ux = R[5];
+      sa.uy = R[6];
+      sa.uz = R[7];
+      sa.dxx = SR[0];
+      sa.dyy = SR[1];
+      sa.dxy = SR[2];
+      sa.hnum = SR[3];
+      sa.pp = point_params();
+      sa.n3 = (long long)N * N * N;
+      sa.n = N;
+      surface_prep_kernel<T><<<dim3(592, p.batch), 256, 0, stream>>>(sa);
+      SHB_CUDA(cudaGetLastError());
+      ++launches;
+      if ((rc = step_async(1))) return rc;  // R[0] now holds psi^{n+1}
+      surface_scan_kernel<T><<<dim3((N * N + 127) / 128, p.batch), 128, 0, stream>>>(
+          R[0], SR[0], SR[1], SR[3], SR[2], N, d_zout, d_surf[0], d_surf[1], d_surf[2]);
+      SHB_CUDA(cudaGetLastError());
+      ++launches;
+      SHB_CUDA(cudaMemcpyAsync(z, d_zout, nc * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(vn, d_surf[0], nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(hh, d_surf[1], nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(kk, d_surf[2], nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaStreamSynchronize(stream));
+      return SH_OK;
+    }
   }
 };
 

@@ -41,7 +41,7 @@ class Params:
     sub_sigma: float = 0.0
     sub_z0: float = 1e-4
     eps_per_replica: tuple | None = None
-    variant: int = 0                 # plane-pass cluster size override (0 = default)
+    variant: int = 0                 # plane-pass cluster size (0 = default, -1 = autotune)
 
     @staticmethod
     def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":
@@ -73,6 +73,9 @@ class Solver:
 
     def __init__(self, params: Params):
         self.lib = L.load()
+        if params.variant < 0:
+            from .autotune import best_variant
+            params = dataclasses.replace(params, variant=best_variant(dataclasses.replace(params, variant=0)))
         self.params = params
         cp, keep = params.to_c()
         h = C.c_void_p()
@@ -178,6 +181,35 @@ class Solver:
         cnt = C.c_int()
         self._chk(self.lib.sh_l1(self.h, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cnt)))
         return out, cnt.value
+
+    def surface_step(self):
+        """surfTrack pass: one advected step; per (x, y) column of the new psi the
+        first crossing z (-1 if none), v_n, H and K (NaN if none)."""
+        n, b = self.params.n, self.params.batch
+        shape = (b, n, n) if b > 1 else (n, n)
+        z = np.empty(shape, dtype=np.int32)
+        vn = np.empty(shape, dtype=np.float64)
+        hh = np.empty(shape, dtype=np.float64)
+        kk = np.empty(shape, dtype=np.float64)
+        self._chk(self.lib.sh_surface_step(self.h, z.ctypes.data_as(C.POINTER(C.c_int)),
+                                           vn.ctypes.data_as(C.POINTER(C.c_double)),
+                                           hh.ctypes.data_as(C.POINTER(C.c_double)),
+                                           kk.ctypes.data_as(C.POINTER(C.c_double))))
+        return z, vn, hh, kk
+
+    def adjoint(self, psi0: np.ndarray, nsteps: int, dl_dpsi_t: np.ndarray, ckpt_every: int = 50):
+        """Discrete adjoint of the CNAB2 loop: returns (dL/d eps, dL/d q0, dL/d psi0)
+        per replica for a loss with gradient dl_dpsi_t at psi^T."""
+        a = np.ascontiguousarray(psi0, dtype=np.float64)
+        g = np.ascontiguousarray(dl_dpsi_t, dtype=np.float64)
+        b = self.params.batch
+        ge = np.empty(b, dtype=np.float64)
+        gq = np.empty(b, dtype=np.float64)
+        gp = np.empty(self.shape, dtype=np.float64)
+        self._chk(self.lib.sh_adjoint(self.h, a.ctypes.data, int(nsteps), g.ctypes.data, int(ckpt_every),
+                                      ge.ctypes.data_as(C.POINTER(C.c_double)),
+                                      gq.ctypes.data_as(C.POINTER(C.c_double)), gp.ctypes.data))
+        return ge, gq, gp
 
     def checkpoint(self) -> bytes:
         size = C.c_size_t()

@@ -92,6 +92,15 @@ def neumann_l1():
     return _pack(p, psi0=psi0, psi=o.psi, steps=20, l1=O.l1_monitor(o.psi, prev, p.dt))
 
 
+def periodic_advected():
+    n = 16
+    p = O.Params(n=n, dt=0.01, eps=-0.7)
+    psi0 = ic.pf3d_lamellae(n, p.dx, kmin=1, kmax=15) + ic.noise(n, 6, 0.05)
+    o = O.PeriodicOracle(psi0, p, advect=True)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10, advect=True, energy=O.energy_spectral_periodic(o.psi, p))
+
+
 CASES = {
     "periodic_plain_16": periodic_plain,
     "periodic_lamellae_32": periodic_lamellae_ref_ic,
@@ -99,6 +108,7 @@ CASES = {
     "periodic_penalty_16": periodic_penalty,
     "neumann_hyperboloid_16": neumann_hyperboloid,
     "neumann_l1_32": neumann_l1,
+    "periodic_advected_16": periodic_advected,
 }
 
 

@@ -50,10 +50,12 @@ def golden(name):
     ("periodic_penalty_16", "periodic"),
     ("neumann_hyperboloid_16", "neumann"),
     ("neumann_l1_32", "neumann"),
+    ("periodic_advected_16", "periodic"),
 ])
 def test_golden_vectors(name, boundary, prec):
     d, kw = golden(name)
     p = S.Params(boundary=boundary, precision=prec, **{k: v for k, v in kw.items() if k in S.Params.__dataclass_fields__})
+    p.advection = bool(d["advect"]) if "advect" in d.files else False
     if "l1" in d.files:
         p.l1_interval = int(d["steps"])
     with S.Solver(p) as s:
@@ -273,3 +275,181 @@ def test_run_host_roundtrip_matches_steps():
         s.step(10)
         b = s.get_psi()
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [16, 32, 64, 128])
+def test_advected_matches_oracle(n, prec):
+    """Periodic step with the Fourier Stokes advection (periodicFFT/pf3d.cpp:395-485)."""
+    p = S.Params(n=n, advection=True, precision=prec, dt=0.01, eps=-0.7, eta=1.0, rho=1.0)
+    psi0 = S.ic.pf3d_lamellae(n, p.dx, kmin=1, kmax=n - 1) + S.ic.noise(n, 21, 0.05)
+    orc = O.PeriodicOracle(psi0, oracle_params(p), advect=True)
+    steps = 20 if n <= 64 else 5
+    orc.run(steps)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(steps)
+        assert rel(s.get_psi(), orc.psi) <= TOL[prec]
+        eo = O.energy_spectral_periodic(orc.psi, oracle_params(p))
+        assert abs(s.energy()[0] - eo) <= ETOL[prec] * abs(eo)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+def test_advected_256_undulated_lamellae(prec):
+    """The advected 256^3 workload's own IC, a few steps against the oracle."""
+    n = 256
+    p = S.Params(n=n, advection=True, precision=prec, dt=0.02)
+    psi0 = S.ic.undulated_lamellae(n, p.dx, seed=0)
+    orc = O.PeriodicOracle(psi0, oracle_params(p), advect=True)
+    orc.run(2)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(2)
+        assert rel(s.get_psi(), orc.psi) <= TOL[prec]
+
+
+def test_advected_checkpoint_roundtrip():
+    n = 32
+    p = S.Params(n=n, advection=True, precision="fp64", dt=0.01)
+    with S.Solver(p) as s:
+        s.set_psi(S.ic.noise(n, 22, 0.5))
+        s.step(3)
+        blob = s.checkpoint()
+        s.step(4)
+        a = s.get_psi()
+        s.restore(blob)
+        s.step(4)
+        b = s.get_psi()
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [32, 64])
+def test_surface_step_matches_oracle(n, prec):
+    """surfTrack (periodicFFT/surfTrack.cpp:592-626, 767-806): crossing z of the new
+    psi per column, with v_n, H and K from the fields of the step."""
+    p = S.Params(n=n, advection=True, precision=prec, dt=0.02, eps=-0.7)
+    # lamellae undulated along x and y, so that both curvatures are non-zero
+    c = np.arange(n) * p.dx
+    lam = n / 2 * p.dx
+    # (off-grid phases: no exact zeros of psi on grid points, whose sign rounding would decide)
+    h = 0.83 * p.dx * (np.sin(2 * np.pi * c / lam + 0.3)[:, None, None] + np.cos(2 * np.pi * c / lam + 0.7)[None, :, None])
+    psi0 = 1.3 * np.cos(c[None, None, :] - h - 0.37)
+    orc = O.PeriodicOracle(psi0, oracle_params(p), advect=True)
+    orc.run(3)
+    orc.step()
+    zo, vo, ho, ko = O.surface_scan(orc.psi, *orc.surface_fields())
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(3)
+        z, vn, hh, kk = s.surface_step()
+        assert rel(s.get_psi(), orc.psi) <= TOL[prec]
+    found = zo >= 0
+    assert found.mean() > 0.9
+    same = z == zo
+    assert same.mean() >= (1.0 if prec == "fp64" else 0.99)
+    m = same & found
+    # FP32: d_t psi = eps psi - L psi + N cancels O(1) terms down to O(0.05)
+    tol = 1e-8 if prec == "fp64" else 1e-3
+    for got, ref in ((vn, vo), (hh, ho), (kk, ko)):
+        scale = max(np.abs(ref[m]).max(), 1e-3)
+        assert np.abs(got[m] - ref[m]).max() <= tol * scale
+    assert np.abs(ko[m]).max() > 1e-4  # the IC really is doubly curved
+    assert np.isnan(vn[~(z >= 0)]).all()
+
+
+def test_surface_step_needs_advection():
+    with S.Solver(S.Params(n=16)) as s:
+        s.set_psi(S.ic.noise(16, 1))
+        with pytest.raises(S.ShError) as e:
+            s.surface_step()
+        assert e.value.code == L.SH_EINVAL
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n,steps,k", [(16, 10, 4), (32, 12, 5), (32, 7, 50)])
+def test_adjoint_matches_oracle(n, steps, k, prec):
+    """Discrete adjoint of CNAB2 (checkpoints every k steps) against the FP64 oracle
+    adjoint, for L = 1/2 ||psi_T - target||^2 with a lamellar target 0.5 cos(1.05 z)."""
+    p = S.Params(n=n, precision=prec, dt=0.05)
+    psi0 = S.ic.noise(n, 31, 0.1) + 1.2 * np.cos(np.arange(n) * p.dx)[None, None, :]
+    target = 0.5 * np.broadcast_to(np.cos(1.05 * np.arange(n) * p.dx)[None, None, :], (n, n, n))
+    loss, ge, gq, gpsi = O.adjoint_gradients_periodic(psi0, oracle_params(p), steps, target)
+    orc = O.PeriodicOracle(psi0, oracle_params(p))
+    orc.run(steps)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(steps)
+        psi_t = s.get_psi()
+        g_e, g_q, g_p = s.adjoint(psi0, steps, psi_t - target, ckpt_every=k)
+    tol = 1e-9 if prec == "fp64" else 1e-4
+    assert abs(g_e[0] - ge) <= tol * abs(ge)
+    assert abs(g_q[0] - gq) <= tol * abs(gq)
+    assert rel(g_p, gpsi) <= tol
+
+
+def test_adjoint_finite_differences_fp32_forward():
+    """FP32 forward + FP64 gradient accumulation against central differences of the
+    FP64 oracle loss (h = 1e-4), as the differentiation workload asks."""
+    import dataclasses
+    n, steps = 16, 20
+    p = S.Params(n=n, precision="fp32", dt=0.05)
+    psi0 = S.ic.noise(n, 32, 0.1) + 1.2 * np.cos(np.arange(n) * p.dx)[None, None, :]
+    target = 0.5 * np.broadcast_to(np.cos(1.05 * np.arange(n) * p.dx)[None, None, :], (n, n, n))
+    op = oracle_params(p)
+
+    def lossf(pp):
+        o = O.PeriodicOracle(psi0, pp)
+        o.run(steps)
+        return 0.5 * ((o.psi - target) ** 2).sum()
+
+    h = 1e-4
+    fe = (lossf(dataclasses.replace(op, eps=op.eps + h)) - lossf(dataclasses.replace(op, eps=op.eps - h))) / (2 * h)
+    fq = (lossf(dataclasses.replace(op, q0=op.q0 + h)) - lossf(dataclasses.replace(op, q0=op.q0 - h))) / (2 * h)
+    orc = O.PeriodicOracle(psi0, op)
+    orc.run(steps)
+    with S.Solver(p) as s:
+        g_e, g_q, _ = s.adjoint(psi0, steps, orc.psi - target, ckpt_every=5)
+    assert abs(g_e[0] - fe) <= 1e-4 * abs(fe)
+    assert abs(g_q[0] - fq) <= 1e-4 * abs(fq)
+
+
+def test_adjoint_batched_replicas():
+    n, steps, b = 16, 8, 3
+    eps = (-0.9, -0.7, -0.5)
+    p = S.Params(n=n, batch=b, precision="fp64", eps_per_replica=eps)
+    psi0 = S.ic.noise_batch(n, (40, 41, 42), 0.3)
+    lam = S.ic.noise_batch(n, (43, 44, 45), 1.0)
+    with S.Solver(p) as s:
+        g_e, g_q, g_p = s.adjoint(psi0, steps, lam, ckpt_every=3)
+    for r in range(b):
+        with S.Solver(S.Params(n=n, precision="fp64", eps=eps[r])) as s1:
+            e1, q1, p1 = s1.adjoint(psi0[r], steps, lam[r], ckpt_every=8)
+        assert abs(g_e[r] - e1[0]) <= 1e-10 * abs(e1[0])
+        assert abs(g_q[r] - q1[0]) <= 1e-10 * abs(q1[0])
+        assert rel(g_p[r], p1) <= 1e-10
+
+
+def test_graph_replay_matches_direct_launches():
+    """Steps replayed from the captured CUDA graph equal steps launched one by one."""
+    n = 64
+    psi0 = S.ic.noise(n, 50)
+    with S.Solver(S.Params(n=n, precision="fp32")) as a, S.Solver(S.Params(n=n, precision="fp32", l1_interval=1000)) as b:
+        a.set_psi(psi0)
+        b.set_psi(psi0)
+        a.step(40)          # 2 graph chunks of 16 + 8 direct steps
+        b.step(40)          # L1 bookkeeping forces direct launches
+        assert a.steps_taken == b.steps_taken == 40
+        assert np.array_equal(a.get_psi(), b.get_psi())
+        assert a.kernel_launches == b.kernel_launches
+
+
+def test_autotune_picks_a_built_variant(tmp_path, monkeypatch):
+    from smectic3d_b200 import autotune
+    monkeypatch.setenv("SMECTIC_B200_CACHE", str(tmp_path / "tuned.json"))
+    p = S.Params(n=64, batch=8, precision="fp32")
+    rec = autotune.tune(p, steps=5)
+    assert rec["variant"] in autotune.CANDIDATES[64]
+    assert (tmp_path / "tuned.json").exists()
+    with S.Solver(S.Params(n=64, batch=8, precision="fp32", variant=-1)) as s:
+        assert s.params.variant == rec["variant"]
