@@ -137,6 +137,22 @@ def traffic_record(kernel_key):
     return json.load(open(path)).get(kernel_key)
 
 
+def max_over_ranks(x, torch, dist, device="cuda"):
+    """Largest value of x over all ranks (the job time is the slowest rank's)."""
+    if dist is None:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, ms_per_rank, torch, dist, device="cuda"):
+    """Whole-job throughput: units of every rank over the slowest rank's time."""
+    world = dist.get_world_size() if dist is not None else 1
+    ms = max_over_ranks(ms_per_rank, torch, dist, device)
+    return world * units_per_rank / (ms / 1e3), ms
+
+
 def timed_steps(solver, k, torch, dist):
     ext = torch.cuda.ExternalStream(solver.stream)
     start = torch.cuda.Event(enable_timing=True)
@@ -151,12 +167,7 @@ def timed_steps(solver, k, torch, dist):
     end.synchronize()
     solver.synchronize()
     torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    if dist is not None:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    return ms
+    return max_over_ranks(start.elapsed_time(end), torch, dist)
 
 
 def run_ours(args, rank, world, local_rank, dist):
@@ -238,11 +249,7 @@ def run_ours(args, rank, world, local_rank, dist):
     t0 = time.perf_counter()
     se.run(host_in, k, host_out)
     t1 = time.perf_counter()
-    e2e_s = t1 - t0
-    if dist is not None:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(t1 - t0, torch, dist)
     se.close()
     S.load_library().sh_host_free(hp_in)
     S.load_library().sh_host_free(hp_out)
@@ -305,7 +312,7 @@ def adjoint_ratio(args, torch):
         s.step(t_steps)
         t_fwd = time.perf_counter() - t0
         lam = s.get_psi() - target
-        s.adjoint(psi0, 10, lam, ckpt_every=5)  # warm the adjoint kernels
+        s.adjoint(psi0, t_steps, lam, ckpt_every=k)  # warm: kernels and the adjoint's buffers
         t0 = time.perf_counter()
         ge, gq, _ = s.adjoint(psi0, t_steps, lam, ckpt_every=k)
         t_adj = time.perf_counter() - t0

@@ -18,6 +18,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "libsmectic_b200.so"
+DRIVER = PKG / "smectic_run"
 INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -33,6 +34,19 @@ def nvcc() -> str:
 
 def sources():
     return sorted(CSRC.glob("*.cu"))
+
+
+def build_driver() -> Path:
+    """g++ build of the host driver smectic_run against the in-tree library."""
+    src = CSRC / "smectic_run.cpp"
+    if DRIVER.exists() and DRIVER.stat().st_mtime > max(src.stat().st_mtime, LIB.stat().st_mtime):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", f"-I{INCLUDE}", str(src), "-o", str(DRIVER), f"-L{PKG}", "-lsmectic_b200",
+           "-Wl,-rpath,$ORIGIN"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"driver build failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    return DRIVER
 
 
 def headers():
@@ -73,6 +87,7 @@ def build(verbose: bool = False, ptxas_info: bool = False, jobs: int | None = No
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    build_driver()
     return LIB
 
 

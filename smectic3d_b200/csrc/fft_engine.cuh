@@ -40,6 +40,33 @@ template <typename T>
 __device__ __forceinline__ cplx<T> cadd(cplx<T> a, cplx<T> b) { return mk<T>(a.x + b.x, a.y + b.y); }
 template <typename T>
 __device__ __forceinline__ cplx<T> csub(cplx<T> a, cplx<T> b) { return mk<T>(a.x - b.x, a.y - b.y); }
+
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 1000 && !defined(SHB_NO_F32X2)
+// sm_100 packed FP32x2 arithmetic: one instruction for both lanes of a complex
+// float, each lane rounded to nearest exactly as the scalar FADD / FSUB
+__device__ __forceinline__ unsigned long long pk2(float2 v) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(v.x), "f"(v.y));
+  return r;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+template <>
+__device__ __forceinline__ float2 cadd<float>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+template <>
+__device__ __forceinline__ float2 csub<float>(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+#endif
 template <typename T>
 __device__ __forceinline__ cplx<T> cmul(cplx<T> a, cplx<T> b) {
   return mk<T>(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));

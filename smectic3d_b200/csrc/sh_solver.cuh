@@ -111,6 +111,23 @@ struct Solver final : SolverBase {
   int* d_zout = nullptr;
   double* d_surf[3] = {nullptr, nullptr, nullptr};
   bool real_fields_current = false;
+  // adjoint work buffers, kept for the handle's lifetime once allocated
+  struct AdjBufs {
+    cplx<T>* ck = nullptr;   // checkpoints: nseg states x {W, P, Nt}
+    cplx<T>* hs = nullptr;   // (k+1) psihat of a segment, pencil-major
+    T* hr = nullptr;         // (k+1) psi of a segment
+    cplx<T>* lam = nullptr;  // lambdahat, pencil-major
+    cplx<T>* gp = nullptr;   // partial of g
+    cplx<T>* mp = nullptr;   // partial of mu
+    T* mu[2] = {nullptr, nullptr};
+    double* red = nullptr;
+    double* acc = nullptr;
+    int nseg = 0, k = 0;
+    ~AdjBufs() {
+      cudaFree(ck); cudaFree(hs); cudaFree(hr); cudaFree(lam); cudaFree(gp); cudaFree(mp);
+      cudaFree(mu[0]); cudaFree(mu[1]); cudaFree(red); cudaFree(acc);
+    }
+  } adj;
   // adjoint: per-step history of a recomputed segment (psihat pencil-major, psi real)
   cplx<T>* hist_spec = nullptr;
   T* hist_real = nullptr;
@@ -543,21 +560,7 @@ struct Solver final : SolverBase {
       const int saved_l1 = p.l1_interval;
       p.energy_trace = 0;
       p.l1_interval = 0;
-      struct Bufs {
-        cplx<T>* ck = nullptr;   // nseg states x {W, P, Nt}
-        cplx<T>* hs = nullptr;   // (K+1) psihat
-        T* hr = nullptr;         // (K+1) psi
-        cplx<T>* lam = nullptr;  // lambdahat, pencil-major
-        cplx<T>* gp = nullptr;   // partial of g
-        cplx<T>* mp = nullptr;   // partial of mu
-        T* mu[2] = {nullptr, nullptr};
-        double* red = nullptr;
-        double* acc = nullptr;
-        ~Bufs() {
-          cudaFree(ck); cudaFree(hs); cudaFree(hr); cudaFree(lam); cudaFree(gp); cudaFree(mp);
-          cudaFree(mu[0]); cudaFree(mu[1]); cudaFree(red); cudaFree(acc);
-        }
-      } bf;
+      AdjBufs& bf = adj;
       auto restore = [&]() { p.energy_trace = saved_trace; p.l1_interval = saved_l1; hist_spec = nullptr; hist_real = nullptr; };
 #define ADJ_CUDA(expr)                                                           \
   do {                                                                           \
@@ -575,16 +578,33 @@ struct Solver final : SolverBase {
       return rc;           \
     }                      \
   } while (0)
-      ADJ_CUDA(cudaMalloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
-      ADJ_CUDA(cudaMalloc(&bf.hs, size_t(K + 1) * fe * sizeof(cplx<T>)));
-      ADJ_CUDA(cudaMalloc(&bf.hr, size_t(K + 1) * nr * sizeof(T)));
-      ADJ_CUDA(cudaMalloc(&bf.lam, fe * sizeof(cplx<T>)));
-      ADJ_CUDA(cudaMalloc(&bf.gp, fe * sizeof(cplx<T>)));
-      ADJ_CUDA(cudaMalloc(&bf.mp, fe * sizeof(cplx<T>)));
-      ADJ_CUDA(cudaMalloc(&bf.mu[0], nr * sizeof(T)));
-      ADJ_CUDA(cudaMalloc(&bf.mu[1], nr * sizeof(T)));
-      ADJ_CUDA(cudaMalloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
-      ADJ_CUDA(cudaMalloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
+      // buffers persist across calls; they grow when nsteps / ckpt_every need more
+      if (bf.nseg < nseg) {
+        cudaFree(bf.ck);
+        bf.ck = nullptr;
+        bf.nseg = 0;
+        ADJ_CUDA(cudaMalloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
+        bf.nseg = nseg;
+      }
+      if (bf.k < K) {
+        cudaFree(bf.hs);
+        cudaFree(bf.hr);
+        bf.hs = nullptr;
+        bf.hr = nullptr;
+        bf.k = 0;
+        ADJ_CUDA(cudaMalloc(&bf.hs, size_t(K + 1) * fe * sizeof(cplx<T>)));
+        ADJ_CUDA(cudaMalloc(&bf.hr, size_t(K + 1) * nr * sizeof(T)));
+        bf.k = K;
+      }
+      if (!bf.lam) {
+        ADJ_CUDA(cudaMalloc(&bf.lam, fe * sizeof(cplx<T>)));
+        ADJ_CUDA(cudaMalloc(&bf.gp, fe * sizeof(cplx<T>)));
+        ADJ_CUDA(cudaMalloc(&bf.mp, fe * sizeof(cplx<T>)));
+        ADJ_CUDA(cudaMalloc(&bf.mu[0], nr * sizeof(T)));
+        ADJ_CUDA(cudaMalloc(&bf.mu[1], nr * sizeof(T)));
+        ADJ_CUDA(cudaMalloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
+        ADJ_CUDA(cudaMalloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
+      }
       ADJ_CUDA(cudaMemsetAsync(bf.acc, 0, size_t(p.batch) * 4 * sizeof(double), stream));
       const size_t fb = fe * sizeof(cplx<T>);
       // ---- forward sweep with checkpoints at s = 0, K, 2K, ...

@@ -1,0 +1,40 @@
+"""Run a few time steps of one configuration: the command that ncu captures.
+
+    python -m smectic3d_b200.profile_run --boundary neumann --precision fp32 --n 256 --steps 4
+
+It sets a seeded U(-0.1, 0.1) field, takes ``--steps`` steps and exits. The
+kernel order per step is pencil (x) then plane (y,z), after one init plane and
+one init pencil launch. ``ncu -k regex:plane_kernel -s 2 -c 1`` therefore
+captures the plane pass of the second step.
+"""
+from __future__ import annotations
+
+import argparse
+
+from .ic import noise
+from .solver import Params, Solver
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--boundary", default="neumann", choices=["periodic", "neumann"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4)
+    ap.add_argument("--variant", type=int, default=0)
+    ap.add_argument("--advection", action="store_true")
+    args = ap.parse_args(argv)
+    p = Params(n=args.n, batch=args.batch, boundary=args.boundary, precision=args.precision, variant=args.variant,
+               advection=args.advection)
+    with Solver(p) as s:
+        import numpy as np
+        psi = np.stack([noise(args.n, r) for r in range(args.batch)]) if args.batch > 1 else noise(args.n, 0)
+        s.set_psi(psi)
+        s.step(args.steps)
+        s.synchronize()
+    print("ok")
+
+
+if __name__ == "__main__":
+    main()
