@@ -76,47 +76,80 @@ def algorithmic_bytes(boundary, n, batch, precision):
 # clocks
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock and throttle reasons sampled every 10 ms by an NVML thread
+    while the timed region runs (read-only NVML queries); the GPU is found
+    by its UUID so CUDA_VISIBLE_DEVICES remapping does not matter."""
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+    def __init__(self, cuda_index, period=0.01):
+        import threading
+        self.cuda_index = cuda_index
+        self.period = period
+        self.samples = []          # (t, sm_mhz, reasons bitmask)
+        self.window = None
+        self.smax = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        try:
+            uuid = str(torch.cuda.get_device_properties(self.cuda_index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
+
+    def _run(self, nv, h):
+        get_r = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                self.samples.append((time.perf_counter(), nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), get_r(h)))
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(suffix=".csv")
-        os.close(fd)
+        import threading
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            nv, h = self._handle()
+            self.smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception:
+            return
+        self._nvml = nv
+        self._thread = threading.Thread(target=self._run, args=(nv, h), daemon=True)
+        self._thread.start()
+        t0 = time.perf_counter()
+        while not self.samples and time.perf_counter() - t0 < 2.0:
+            time.sleep(0.002)
+
+    def begin(self):
+        self.window = [time.perf_counter(), None]
+
+    def end(self):
+        if self.window:
+            self.window[1] = time.perf_counter()
 
     def stop(self):
-        if self.proc is None:
+        if self._thread is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = []
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) >= 9:
-                rows.append(f)
-        os.unlink(self.path)
+        self._stop.set()
+        self._thread.join(timeout=2)
+        lo, hi = self.window if self.window and self.window[1] else (-math.inf, math.inf)
+        rows = [s for s in self.samples if lo <= s[0] <= hi]
+        if not rows:   # region shorter than the period: the samples either side
+            before = [s for s in self.samples if s[0] < lo][-1:]
+            after = [s for s in self.samples if s[0] > hi][:1]
+            rows = before + after
         if not rows:
             return None
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        reasons = sorted({k for _, _, m in rows for k, bit in self.REASONS.items() if m & bit})
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": self.smax, "reasons": reasons,
+                "samples": len(rows), "source": "nvml, 10 ms"}
 
 
 # ---------------------------------------------------------------------------
@@ -153,7 +186,7 @@ def aggregate_rate(units_per_rank, ms_per_rank, torch, dist, device="cuda"):
     return world * units_per_rank / (ms / 1e3), ms
 
 
-def timed_steps(solver, k, torch, dist):
+def timed_steps(solver, k, torch, dist, clocks=None):
     ext = torch.cuda.ExternalStream(solver.stream)
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
@@ -161,12 +194,18 @@ def timed_steps(solver, k, torch, dist):
         dist.barrier()
     solver.synchronize()
     torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.begin()
     start.record(ext)
     solver.step_async(k)
     end.record(ext)
     end.synchronize()
+    if clocks is not None:
+        clocks.end()
     solver.synchronize()
     torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
     return max_over_ranks(start.elapsed_time(end), torch, dist)
 
 
@@ -189,7 +228,7 @@ def run_ours(args, rank, world, local_rank, dist):
     l0 = s32.kernel_launches
     clocks = ClockSampler(local_rank)
     clocks.start()
-    ms = timed_steps(s32, k, torch, dist)
+    ms = timed_steps(s32, k, torch, dist, clocks)
     clk = clocks.stop()
     launches = s32.kernel_launches - l0
     value = world * k / (ms / 1e3)
