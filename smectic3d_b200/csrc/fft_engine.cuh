@@ -162,10 +162,12 @@ void host_twiddles(Vec& out) {
   }
 }
 
-// copy the device table into shared memory (caller syncs)
+// copy the first ``count`` entries of the device table into shared memory
+// (caller syncs); the periodic transforms stop before the quarter-wave part
 template <typename T, int N>
-__device__ __forceinline__ TwTables<T> stage_twiddles(cplx<T>* smem, const cplx<T>* __restrict__ g, int tid, int nthr) {
-  for (int i = tid; i < tw_total<N>(); i += nthr) smem[i] = __ldg(&g[i]);
+__device__ __forceinline__ TwTables<T> stage_twiddles(cplx<T>* smem, const cplx<T>* __restrict__ g, int tid, int nthr,
+                                                      int count = tw_total<N>()) {
+  for (int i = tid; i < count; i += nthr) smem[i] = __ldg(&g[i]);
   TwTables<T> t;
   t.f = smem;
   t.i = smem + tw_size<N, -1>();

@@ -51,6 +51,11 @@ struct PencilCfg {
   static constexpr size_t tw_off(int mode) { return SET_BYTES * pencil_sets(mode); }
   static constexpr size_t red_off(int mode) { return tw_off(mode) + size_t(tw_total<N>()) * sizeof(cplx<T>); }
   static constexpr size_t smem(int mode) { return red_off(mode) + 64 * sizeof(double); }
+  // The FP32 step runs three 256-thread CTAs per SM (at most 85 registers a
+  // thread); every other launch leaves the register budget to ptxas (0).
+  static constexpr int min_blocks(int mode) {
+    return (sizeof(T) == 4 && mode == kPencilStep && THREADS == 256) ? 3 : 0;
+  }
   static_assert(FP % TK == 0, "tile must divide the plane");
   static_assert(THREADS % 32 == 0, "pencil CTA must be whole warps");
 };
@@ -191,7 +196,7 @@ __device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 
 template <typename T, int N, bool DCT, int MODE>
-__global__ void __launch_bounds__(PencilCfg<T, N, DCT>::THREADS)
+__global__ void __launch_bounds__(PencilCfg<T, N, DCT>::THREADS, PencilCfg<T, N, DCT>::min_blocks(MODE))
 pencil_kernel(PencilArgs<T> a) {
   using Cfg = PencilCfg<T, N, DCT>;
   using Ops = PencilOps<T, N, DCT>;
@@ -234,14 +239,15 @@ pencil_kernel(PencilArgs<T> a) {
 
   if constexpr (MODE == kPencilStep || MODE == kPencilStepAdv) {
     Ops::load_tile(buf, a.src + plane_base, f0);
-    // the state W of this line, fetched while the transform runs
+    __syncthreads();
+    Ops::forward(v, L, t, tw);
+    // the state W of this line, loaded after the transform: holding it through
+    // the transform costs the registers of a third resident CTA
     cplx<T> wreg[E];
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
       for (int r = 0; r < RL; ++r) wreg[b * RL + r] = wrow[out_index<N, -1>(t, b, r)];
-    __syncthreads();
-    Ops::forward(v, L, t, tw);
     // mode-independent constants of the update; the (ky, kz) part of |q|^2 is
     // fixed for the line
     const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha);

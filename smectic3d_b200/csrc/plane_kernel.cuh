@@ -35,7 +35,6 @@ enum RealOp : int {
   kOpAdvected = 1,  // N(in[0]) + penalty - sum_i in[4+i] in[1+i]  (nonlinearity with -u.grad psi)
 };
 
-__host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 template <typename T, int N, int CL, bool DCT>
 struct PlaneCfg {
@@ -44,7 +43,7 @@ struct PlaneCfg {
   static constexpr int NC = N / (2 * CL);
   static constexpr int THREADS = NC * G;
   static constexpr int LS = line_stride(N);
-  static constexpr int LINES = NC + 1;
+  static constexpr int LINES = DCT ? NC : NC + 1;  // periodic: + the kz = N/2 column
   static constexpr int ROWS = N / CL;
   static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
   static constexpr int RL_INV = radix_of<N, +1, Plan<N>::P - 1>();
@@ -62,13 +61,28 @@ struct PlaneCfg {
   static constexpr int BLK = ((BLK_A > BLK_B ? BLK_A : BLK_B) + 1) / 2 * 2;  // even: 16-byte blocks
   static constexpr size_t LB_BYTES = align_up(size_t(LINES) * LS * sizeof(cplx<T>), 128);
   static constexpr size_t XB_BYTES = CL > 1 ? align_up(size_t(CL) * BLK * sizeof(cplx<T>), 128) : 0;
-  static constexpr size_t SB_OFF = LB_BYTES;
-  static constexpr size_t RB_OFF = SB_OFF + XB_BYTES;
+  // With a cluster the line buffer and the send blocks share memory: the
+  // transform scratch of a phase is never live while the send blocks of the
+  // neighbouring exchange are (a barrier, and a wait for the outgoing copies,
+  // separates them).
+  static constexpr bool ALIAS = CL > 1;
+  static constexpr size_t SB_OFF = ALIAS ? 0 : LB_BYTES;
+  static constexpr size_t RB_OFF = ALIAS ? (LB_BYTES > XB_BYTES ? LB_BYTES : XB_BYTES) : SB_OFF + XB_BYTES;
   static constexpr size_t TW_OFF = RB_OFF + XB_BYTES;
-  static constexpr size_t MB_OFF = align_up(TW_OFF + size_t(tw_total<N>()) * sizeof(cplx<T>), 16);
+  // the periodic transforms need no quarter-wave table
+  static constexpr int TW_ENTRIES = tw_total<N>() - (DCT ? 0 : N);
+  static constexpr size_t MB_OFF = align_up(TW_OFF + size_t(TW_ENTRIES) * sizeof(cplx<T>), 16);
   static constexpr size_t RED_OFF = MB_OFF + 16;
   static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
   static constexpr bool fits = SMEM <= 227 * 1024;  // per-CTA shared memory limit of sm_100
+  // Three resident CTAs need SMEM <= (228 KB - 3 x 1 KB reserved) / 3 and at
+  // most 85 registers a thread; ptxas is asked for the latter only where the
+  // former holds (FP32 clusters of 256-thread CTAs).
+#ifndef SHB_PLANE_THREE
+#define SHB_PLANE_THREE 1
+#endif
+  static constexpr int MIN_BLOCKS =
+      (SHB_PLANE_THREE && sizeof(T) == 4 && CL > 1 && THREADS == 256 && SMEM <= 76800) ? 3 : 0;
   static_assert(THREADS % 32 == 0, "plane CTA must be whole warps");
 };
 
@@ -119,9 +133,6 @@ __device__ __forceinline__ uint32_t dsmem_map(const void* p, int rank) {
   asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
   return r;
 }
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
 
 // Cluster exchange state: send / receive block arrays, two mbarriers (one per
 // exchange direction) and their phase parities.
@@ -133,24 +144,6 @@ struct Xchg {
   uint32_t phases;
   int* timeout;
 };
-
-__device__ __forceinline__ void mbar_wait_bounded(uint64_t* mbar, uint32_t parity, int* timeout) {
-  const uint32_t a = smem_u32(mbar);
-  const long long t0 = clock64();
-  for (;;) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return;
-    if (clock64() - t0 > (1ll << 31)) {  // about a second: give up, flag it, keep the cluster in step
-      atomicExch(timeout, 1);
-      return;
-    }
-  }
-}
 
 // Every thread has written its share of the send blocks; copy block d to CTA d
 // (cp.async.bulk shared::cta -> shared::cluster, completing on the receiver's
@@ -343,6 +336,7 @@ struct PlaneOps {
         }
       __syncthreads();
     } else {
+      if constexpr (Cfg::ALIAS) __syncthreads();  // every line has left the scratch the send blocks overlay
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -368,6 +362,7 @@ struct PlaneOps {
   // inverse z transform of row pair ``line``; v slot holds psi(y0, z), psi(y0+1, z)
   static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], const cplx<T>* buf, const Xchg<T>& xs,
                                                      cplx<T>* L, int q, int t, const TwTables<T>& tw) {
+    if constexpr (Cfg::ALIAS) send_blocks_free();  // the scratch L overlays the outgoing send blocks
     if constexpr (!DCT) {
       // Z = X_a + i X_b with Hermitian extension; slot 0 holds (X[0], X[N/2])
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
@@ -506,6 +501,7 @@ struct PlaneOps {
   // ---- column phase, forward direction ---------------------------------
   static __device__ void col_forward_store(cplx<T>* buf, const Xchg<T>& xs, cplx<T>* __restrict__ plane, int rank,
                                            const TwTables<T>& tw) {
+    if constexpr (Cfg::ALIAS) send_blocks_free();  // the scratch L overlays the outgoing send blocks
     const int line = threadIdx.x / G, t = threadIdx.x % G;
     cplx<T>* L = buf + line * LS;
     cplx<T> v[E];
@@ -614,7 +610,7 @@ __device__ __forceinline__ void row_nonlin(cplx<T> (&v)[Plan<N>::E], cplx<T>* L,
 }
 
 template <typename T, int N, int CL, bool DCT, int MODE>
-__global__ void __launch_bounds__(PlaneCfg<T, N, CL, DCT>::THREADS)
+__global__ void __launch_bounds__(PlaneCfg<T, N, CL, DCT>::THREADS, PlaneCfg<T, N, CL, DCT>::MIN_BLOCKS)
 plane_kernel(PlaneArgs<T> a) {
   using Cfg = PlaneCfg<T, N, CL, DCT>;
   using Ops = PlaneOps<T, N, CL, DCT>;
@@ -624,7 +620,8 @@ plane_kernel(PlaneArgs<T> a) {
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::RED_OFF);
   const TwTables<T> tw =
-      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS);
+      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS,
+                           Cfg::TW_ENTRIES);
 
   int rank = 0;
   if constexpr (CL > 1) rank = int(cg::this_cluster().block_rank());

@@ -8,6 +8,32 @@
 namespace shb {
 namespace cg = cooperative_groups;
 
+__host__ __device__ constexpr size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Wait for phase ``parity`` of an mbarrier, for about a second at most: on
+// expiry set *timeout and return, so that a lost transfer cannot hang the SM.
+__device__ __forceinline__ void mbar_wait_bounded(uint64_t* mbar, uint32_t parity, int* timeout) {
+  const uint32_t a = smem_u32(mbar);
+  const long long t0 = clock64();
+  for (;;) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return;
+    if (clock64() - t0 > (1ll << 31)) {
+      atomicExch(timeout, 1);
+      return;
+    }
+  }
+}
+
 enum NonlinKind : int { kQuintic = 0, kQuadCubic = 1 };
 enum SchemeKind : int { kCNAB2 = 0, kIMEXEuler = 1 };
 enum PassFlags : int {
