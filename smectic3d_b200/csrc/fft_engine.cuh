@@ -333,6 +333,32 @@ __device__ __forceinline__ void passes_from(cplx<T>* line, cplx<T> (&v)[Plan<N>:
   }
 }
 
+// Mirror partners in registers.  After a forward transform (and before an
+// inverse one) slot b*RL + r of thread t holds element k = t + G b + M r,
+// M = N / RL.  part[slot] receives element (N - k) mod N, which thread
+// (G - t) mod G holds in a compile-time slot: one warp shuffle per component
+// instead of a round trip through shared memory.  Every lane of the warp
+// must call it.
+template <typename T>
+__device__ __forceinline__ cplx<T> shfl_c(cplx<T> v, int src, int width) {
+  return mk<T>(__shfl_sync(0xffffffffu, v.x, src, width), __shfl_sync(0xffffffffu, v.y, src, width));
+}
+template <typename T, int N, int RL>
+__device__ __forceinline__ void mirror_partners(const cplx<T> (&v)[Plan<N>::E], cplx<T> (&part)[Plan<N>::E], int t) {
+  constexpr int E = Plan<N>::E, G = N / E, NB = E / RL;
+  const int src = (G - t) & (G - 1);
+#pragma unroll
+  for (int b = 0; b < NB; ++b)
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      // t != 0: thread G - t, slot (NB - 1 - b, RL - 1 - r)
+      const cplx<T> q = shfl_c<T>(v[(NB - 1 - b) * RL + (RL - 1 - r)], src, G);
+      // t == 0: this thread, slot (NB - b, RL - 1 - r), or (0, (RL - r) mod RL) when b = 0
+      const int zs = b == 0 ? (RL - r) % RL : (NB - b) * RL + (RL - 1 - r);
+      part[b * RL + r] = t == 0 ? v[zs] : q;
+    }
+}
+
 // Full transform.  The first pass reads element i through ld(i); the result of
 // the last pass stays in v (element out_index<N,DIR>(t,b,r) in slot b*R+r).
 // ``tw`` is the pass-major twiddle table of direction DIR (shared memory).

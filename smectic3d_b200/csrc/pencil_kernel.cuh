@@ -114,19 +114,15 @@ struct PencilOps {
       fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(i)]; });
     } else {
       fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return L[pad(i < N / 2 ? 2 * i : 2 * (N - 1 - i) + 1)]; });
-      __syncwarp();
-#pragma unroll
-      for (int b = 0; b < E / RL; ++b)
-#pragma unroll
-        for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
-      __syncwarp();
+      cplx<T> part[E];  // element (N - k) mod N of every slot
+      mirror_partners<T, N, RL>(v, part, t);
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
           cplx<T> w = tw.d[k];
-          v[b * RL + r] = cadd<T>(cmul<T>(L[pad(k)], w), cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w)));
+          v[b * RL + r] = cadd<T>(cmul<T>(v[b * RL + r], w), cmul<T>(part[b * RL + r], conjg<T>(w)));
         }
     }
   }
@@ -144,23 +140,27 @@ struct PencilOps {
 #pragma unroll
         for (int r = 0; r < RLI; ++r) L[pad(out_index<N, +1>(t, b, r))] = v[b * RLI + r];
     } else {
-      __syncwarp();
+      // REDFT01 input exp(+i pi i/2N) (X[i] - i X[N-i]), X[N] = 0, formed in
+      // registers: the first inverse pass reads element i in the slot where
+      // the forward transform left element i
+      cplx<T> part[E];
+      mirror_partners<T, N, RL>(v, part, t);
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
-        for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
-      __syncwarp();
-      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
-        cplx<T> a = L[pad(i)];
-        cplx<T> u = a;
-        if (i != 0) {
-          cplx<T> bb = L[pad(N - i)];
-          u = mk<T>(a.x + bb.y, a.y - bb.x);
+        for (int r = 0; r < RL; ++r) {
+          const int i = out_index<N, -1>(t, b, r);
+          const cplx<T> a = v[b * RL + r];
+          cplx<T> u = a;
+          if (i != 0) {
+            const cplx<T> bb = part[b * RL + r];
+            u = mk<T>(a.x + bb.y, a.y - bb.x);
+          }
+          cplx<T> w = tw.d[i];
+          w.y = -w.y;
+          v[b * RL + r] = cmul<T>(u, w);
         }
-        cplx<T> w = tw.d[i];
-        w.y = -w.y;
-        return cmul<T>(u, w);
-      });
+      fft_regs<T, N, +1>(v, L, t, tw.i);
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RLI; ++b)

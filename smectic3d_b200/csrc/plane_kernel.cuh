@@ -404,12 +404,8 @@ struct PlaneOps {
                                              int line, int t, const TwTables<T>& tw) {
     fft_regs<T, N, -1>(v, L, t, tw.f);
     constexpr int RL = Cfg::RL_FWD;
-    __syncwarp();
-#pragma unroll
-    for (int b = 0; b < E / RL; ++b)
-#pragma unroll
-      for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
-    __syncwarp();
+    cplx<T> part[E];  // element (N - k) mod N of every slot
+    mirror_partners<T, N, RL>(v, part, t);
     if constexpr (!DCT) {
       // split Z into the two half spectra; slot k < N/2 from register r < RL/2
       cplx<T> oa[E / 2], ob[E / 2];
@@ -419,12 +415,13 @@ struct PlaneOps {
         for (int r = 0; r < RL / 2; ++r) {
           const int k = out_index<N, -1>(t, b, r);
           const int s = b * (RL / 2) + r;
+          const cplx<T> zk = v[b * RL + r];
           if (k == 0) {
-            cplx<T> z0 = L[pad(0)], zn = L[pad(N / 2)];
-            oa[s] = mk<T>(z0.x, zn.x);
-            ob[s] = mk<T>(z0.y, zn.y);
+            const cplx<T> zn = v[RL / 2];  // k = N/2 sits in slot (0, RL/2) of the same thread
+            oa[s] = mk<T>(zk.x, zn.x);
+            ob[s] = mk<T>(zk.y, zn.y);
           } else {
-            cplx<T> zk = L[pad(k)], zm = L[pad(N - k)];
+            const cplx<T> zm = part[b * RL + r];
             oa[s] = mk<T>(T(0.5) * (zk.x + zm.x), T(0.5) * (zk.y - zm.y));
             ob[s] = mk<T>(T(0.5) * (zk.y + zm.y), T(0.5) * (zm.x - zk.x));
           }
@@ -457,15 +454,15 @@ struct PlaneOps {
         bulk_exchange<T, CL>(xs, 1, rank, Cfg::BLK);
       }
     } else {
-      cplx<T> o[E];
+      cplx<T>(&o)[E] = v;  // REDFT10 output, in place
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
           cplx<T> w = tw.d[k];
-          cplx<T> a = cmul<T>(L[pad(k)], w);
-          cplx<T> bm = cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w));
+          cplx<T> a = cmul<T>(v[b * RL + r], w);
+          cplx<T> bm = cmul<T>(part[b * RL + r], conjg<T>(w));
           o[b * RL + r] = cadd<T>(a, bm);
         }
       if constexpr (CL == 1) {
@@ -540,6 +537,8 @@ struct PlaneOps {
       }
     } else {
       fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return col_in(buf, xs, line, mk_perm<N>(i)); });
+      // the pairing goes through shared memory here: the register version
+      // spills at three CTAs per SM
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
