@@ -33,9 +33,11 @@ SolverBase* make_solver(int n, int variant) {
       if (cl == 4) return make_if_fits<T, 128, 4, DCT>();
       return nullptr;
     case 256:
+      // default: 8 for FP32 (three CTAs per SM), 16 for FP64 (half the shared
+      // memory of 8, two CTAs per SM)
       if (cl == 4) return make_if_fits<T, 256, 4, DCT>();
-      if (cl == 0 || cl == 8) return make_if_fits<T, 256, 8, DCT>();
-      if (cl == 16) return make_if_fits<T, 256, 16, DCT>();
+      if (cl == 8 || (cl == 0 && sizeof(T) == 4)) return make_if_fits<T, 256, 8, DCT>();
+      if (cl == 16 || (cl == 0 && sizeof(T) == 8)) return make_if_fits<T, 256, 16, DCT>();
       return nullptr;
 #ifdef SHB_WITH_512
     case 512:
