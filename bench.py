@@ -333,14 +333,16 @@ def run_ours(args, rank, world, local_rank, dist):
 def adjoint_ratio(args, torch):
     """Differentiation workload: 128^3 periodic, FP32 forward, FP64 gradient
     accumulation, dt=0.05, checkpoints every 50 steps, L = 1/2 ||psi_T - target||^2
-    with target 0.5 cos(1.05 z).  Times T forward steps and sh_adjoint over the
+    with target 0.5 cos(1.05 z), psi0 = 1.328 cos(z) + U(-0.1, 0.1).  Times T forward steps and sh_adjoint over the
     same T steps (its own forward sweep, the recompute and the reverse sweep)."""
     import numpy as np
     import smectic3d_b200 as S
     n, k = 128, 50
     t_steps = args.adjoint_steps
     p = S.Params(n=n, precision="fp32", dt=0.05, eps=-0.75)
-    psi0 = S.ic.noise(n, 0)
+    # lamellae of the reference amplitude along z, slightly off the target wavenumber, plus noise
+    z = np.arange(n) * p.dx
+    psi0 = 1.328 * np.cos(z)[None, None, :] + S.ic.noise(n, 0)
     target = 0.5 * np.broadcast_to(np.cos(1.05 * np.arange(n) * p.dx)[None, None, :], (n, n, n))
     with S.Solver(p) as s:
         s.set_psi(psi0)
@@ -425,7 +427,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="neumann256", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
-    ap.add_argument("--adjoint-steps", type=int, default=200, help="steps of the adjoint ratio (0 = skip)")
+    ap.add_argument("--adjoint-steps", type=int, default=1000, help="steps of the adjoint ratio (0 = skip)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

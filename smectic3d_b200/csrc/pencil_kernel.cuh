@@ -75,6 +75,7 @@ struct PencilArgs {
   cplx<T>* u3[3];       // Stokes: partial velocity components (may alias s3)
   double* red;          // per-CTA spectral energy partial [rep][grid.x]
   int* nonfinite;       // set to 1 when a new coefficient is NaN/Inf
+  double coef;          // adjoint: c_{n-1} of the emitted mu combination (0 on the last reverse step)
   const T* q;           // wavenumber table (N entries)
   const cplx<T>* tw;    // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
@@ -359,14 +360,24 @@ pencil_kernel(PencilArgs<T> a) {
         for (int r = 0; r < RL; ++r)
           a.spec_out[(size_t(rep) * FP + f) * N + out_index<N, -1>(t, b, r)] = cscale<T>(v[b * RL + r], inv);
     } else if constexpr (!DCT) {
-      // Discrete adjoint of CNAB2 (reverse of psi^{n+1} = A psi^n + B (3 N^n - N^{n-1})):
+      // Discrete adjoint of CNAB2 (reverse of psi^{n+1} = A psi^n + B (c_n N^n - N^{n-1}), c_0 = 2,
+      // c_n = 3):
       //   lambdahat^n = A lambdahat^{n+1} + ghat^n,  mu^n = B lambda^n,
-      //   dL/dtheta += <lambda^{n+1}, F^-1[dt/2 (psihat^n + psihat^{n+1}) / C2 da/dtheta]>
+      //   g^{n-1} = N'(psi^{n-1}) (c_{n-1} mu^n - mu^{n+1}).
+      // The output partial is that combination, scale B (coef lambdahat^n - lambdahat^{n+1}),
+      // so the plane pass of step n-1 reads one field.  The parameter gradients
+      //   dL/dtheta = sum_n <lambda^{n+1}, dt/2 (psihat^n + psihat^{n+1}) / C2 da/dtheta>
+      // are regrouped by psihat^m: step n adds <lambda^{n+1} + [n >= 1] lambda^n, D psihat^n>, and
+      // the first reverse step (spec_b set) also <lambda^{n+1}, D psihat^{n+1}>.
       const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha), h = T(0.5 * a.pp.dt);
       const T qyz = qy * qy + qz0 * qz0;
       const double wgt = ((kz == 0 || kz == N / 2) ? 1.0 : 2.0) / (double(N) * N * N);
       const double dadq0 = 4.0 * a.pp.alpha * a.pp.q0;
-      KahanSum ge, gq;
+      const T coef = T(a.coef);
+      const bool lam_n = a.coef != 0.0;  // n >= 1
+      // a thread's 16 terms are summed plainly (FP64); the per-CTA and
+      // per-step totals are combined in a fixed order
+      double ge = 0.0, gq = 0.0;
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -379,26 +390,35 @@ pencil_kernel(PencilArgs<T> a) {
           const T inv2 = rcp_rn(T(1) - h * al);
           const T am = (T(1) + h * al) * inv2, bm = h * inv2;
           cplx<T> lam = v[b * RL + r];
+          cplx<T> lnext = mk<T>(T(0), T(0));
           if constexpr (MODE == kPencilAdj) {
             const cplx<T> l1 = lreg[b * RL + r];
-            const size_t sidx = (size_t(rep) * FP + f) * N + kx;
-            const cplx<T> pa = a.spec_a[sidx], pb = a.spec_b[sidx];
-            const double dx = double(h) * (double(pa.x) + double(pb.x)) * double(inv2);
-            const double dy = double(h) * (double(pa.y) + double(pb.y)) * double(inv2);
-            const double inner = wgt * (double(l1.x) * dx + double(l1.y) * dy);
-            ge.add(inner);
-            gq.add(inner * dadq0 * double(d));
             lam = mk<T>(am * l1.x + lam.x, am * l1.y + lam.y);
+            const size_t sidx = (size_t(rep) * FP + f) * N + kx;
+            const cplx<T> pa = a.spec_a[sidx];
+            const double wx = double(l1.x) + (lam_n ? double(lam.x) : 0.0);
+            const double wy = double(l1.y) + (lam_n ? double(lam.y) : 0.0);
+            double dot = wx * double(pa.x) + wy * double(pa.y);
+            if (a.spec_b) {
+              const cplx<T> pb = a.spec_b[sidx];
+              dot += double(l1.x) * double(pb.x) + double(l1.y) * double(pb.y);
+            }
+            const double inner = wgt * double(bm) * dot;  // bm = dt/2 / C2
+            ge += inner;
+            gq += inner * double(d);
+            lnext = l1;
           }
           wrow[kx] = lam;
-          v[b * RL + r] = cscale<T>(lam, scale * bm);
+          v[b * RL + r] = cscale<T>(mk<T>(coef * lam.x - lnext.x, coef * lam.y - lnext.y), scale * bm);
         }
       if constexpr (MODE == kPencilAdj) {
-        const double te = block_sum(ge.s, scratch);
-        const double tq = block_sum(gq.s, scratch);
+        // each CTA accumulates into its own slot over the reverse sweep (fixed order)
+        const double te = block_sum(ge, scratch);
+        const double tq = block_sum(gq, scratch);
         if (threadIdx.x == 0) {
-          a.red[(size_t(rep) * gridDim.x + blockIdx.x) * 2 + 0] = te;
-          a.red[(size_t(rep) * gridDim.x + blockIdx.x) * 2 + 1] = tq;
+          double* o = a.red + (size_t(rep) * gridDim.x + blockIdx.x) * 2;
+          o[0] += te;
+          o[1] += tq * dadq0;
         }
       }
     }

@@ -105,7 +105,6 @@ struct PlaneArgs {
   int op;
   const T* real_in[7];
   T* real_out;
-  double coef;  // adjoint: coefficient c_n of mu^{n+1}
 };
 
 // Cluster barrier.  RELEASE orders this thread's earlier shared-memory writes
@@ -692,7 +691,7 @@ plane_kernel(PlaneArgs<T> a) {
         }
       }
     }
-    if (MODE == kPlaneInvReal || MODE == kPlaneAdj || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
+    if (MODE == kPlaneInvReal || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -703,19 +702,18 @@ plane_kernel(PlaneArgs<T> a) {
         }
     }
     if constexpr (MODE == kPlaneAdj) {
-      // g^n = N'(psi^n) (c_n mu^{n+1} - mu^{n+2});  v holds mu^{n+1}
-      const T beta = T(a.pp.beta), gamma = T(a.pp.gamma), c = T(a.coef);
+      // g^n = N'(psi^n) (c_n mu^{n+1} - mu^{n+2}); v holds the bracket (its
+      // partial is what the pencil pass of step n+1 emitted)
+      const T beta = T(a.pp.beta), gamma = T(a.pp.gamma);
       const T* psi = a.real_in[1];
-      const T* mu2 = a.real_in[0];
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const size_t ia = real_off + size_t(y0) * N + Ops::row_z(t, b, r);
           const cplx<T> m = v[b * RL + r];
-          const T ma = mu2 ? mu2[ia] : T(0), mb = mu2 ? mu2[ia + N] : T(0);
-          v[b * RL + r] = mk<T>(nonlin_deriv<T>(psi[ia], beta, gamma, a.pp.nonlin) * (c * m.x - ma),
-                                nonlin_deriv<T>(psi[ia + N], beta, gamma, a.pp.nonlin) * (c * m.y - mb));
+          v[b * RL + r] = mk<T>(nonlin_deriv<T>(psi[ia], beta, gamma, a.pp.nonlin) * m.x,
+                                nonlin_deriv<T>(psi[ia + N], beta, gamma, a.pp.nonlin) * m.y);
         }
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);

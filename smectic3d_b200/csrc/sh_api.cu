@@ -42,7 +42,9 @@ __global__ void finalize_kernel(const double* red_plane, int nbp, const double* 
   }
 }
 
-__global__ void adj_accumulate_kernel(const double* red, int nblocks, double* acc) {
+// Sum of the per-CTA adjoint gradient slots (red[rep][blk][2]) into
+// acc[rep] = {g_eps, 0, g_q0, 0}, compensated, in a fixed order.
+__global__ void adj_reduce_kernel(const double* red, int nblocks, double* acc) {
   __shared__ double scratch[32];
   const int rep = blockIdx.x;
   KahanSum s0, s1;
@@ -54,17 +56,10 @@ __global__ void adj_accumulate_kernel(const double* red, int nblocks, double* ac
   const double tq = block_sum(s1.s, scratch);
   if (threadIdx.x == 0) {
     double* a = acc + size_t(rep) * 4;
-    KahanSum k;
-    k.s = a[0];
-    k.c = a[1];
-    k.add(te);
-    a[0] = k.s;
-    a[1] = k.c;
-    k.s = a[2];
-    k.c = a[3];
-    k.add(tq);
-    a[2] = k.s;
-    a[3] = k.c;
+    a[0] = te;
+    a[1] = 0.0;
+    a[2] = tq;
+    a[3] = 0.0;
   }
 }
 

@@ -26,10 +26,9 @@ namespace shb {
 // what = 0: energy dv (local + alpha/2 norm spec); what = 1: L1 = A / (dt B)
 __global__ void finalize_kernel(const double* red_plane, int nbp, const double* red_spec, int nbs, int what,
                                 double dv, double spec_norm, double alpha, double dt, double* out);
-// Adds the per-CTA (eps, q0) gradient partials of one adjoint step to the
-// running per-replica totals acc[rep][4] = {sum_eps, comp_eps, sum_q0, comp_q0}
-// (Kahan-compensated across steps).
-__global__ void adj_accumulate_kernel(const double* red, int nblocks, double* acc);
+// Sums the per-CTA (eps, q0) gradient slots of the reverse sweep into
+// acc[rep][4] = {g_eps, 0, g_q0, 0}.
+__global__ void adj_reduce_kernel(const double* red, int nblocks, double* acc);
 
 struct SolverBase {
   sh_params p{};
@@ -118,14 +117,13 @@ struct Solver final : SolverBase {
     T* hr = nullptr;         // (k+1) psi of a segment
     cplx<T>* lam = nullptr;  // lambdahat, pencil-major
     cplx<T>* gp = nullptr;   // partial of g
-    cplx<T>* mp = nullptr;   // partial of mu
-    T* mu[2] = {nullptr, nullptr};
-    double* red = nullptr;
+    cplx<T>* mp = nullptr;   // partial of c_n mu^{n+1} - mu^{n+2}
+    double* red = nullptr;   // per-CTA gradient sums of the reverse sweep
     double* acc = nullptr;
     int nseg = 0, k = 0;
     ~AdjBufs() {
       cudaFree(ck); cudaFree(hs); cudaFree(hr); cudaFree(lam); cudaFree(gp); cudaFree(mp);
-      cudaFree(mu[0]); cudaFree(mu[1]); cudaFree(red); cudaFree(acc);
+      cudaFree(red); cudaFree(acc);
     }
   } adj;
   // adjoint: per-step history of a recomputed segment (psihat pencil-major, psi real)
@@ -600,12 +598,10 @@ struct Solver final : SolverBase {
         ADJ_CUDA(cudaMalloc(&bf.lam, fe * sizeof(cplx<T>)));
         ADJ_CUDA(cudaMalloc(&bf.gp, fe * sizeof(cplx<T>)));
         ADJ_CUDA(cudaMalloc(&bf.mp, fe * sizeof(cplx<T>)));
-        ADJ_CUDA(cudaMalloc(&bf.mu[0], nr * sizeof(T)));
-        ADJ_CUDA(cudaMalloc(&bf.mu[1], nr * sizeof(T)));
         ADJ_CUDA(cudaMalloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
         ADJ_CUDA(cudaMalloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
       }
-      ADJ_CUDA(cudaMemsetAsync(bf.acc, 0, size_t(p.batch) * 4 * sizeof(double), stream));
+      ADJ_CUDA(cudaMemsetAsync(bf.red, 0, size_t(p.batch) * QC::TILES * 2 * sizeof(double), stream));
       const size_t fb = fe * sizeof(cplx<T>);
       // ---- forward sweep with checkpoints at s = 0, K, 2K, ...
       ADJ_CUDA(cudaMemcpyAsync(d_psi, psi0, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
@@ -629,11 +625,10 @@ struct Solver final : SolverBase {
         PencilArgs<T> b = pencil_args();
         b.src = bf.gp;
         b.w = bf.lam;
-        b.dst = bf.mp;
+        b.dst = bf.mp;  // partial of c_{T-1} mu^T
+        b.coef = nsteps - 1 >= 1 ? 3.0 : 2.0;
         ADJ_RC(launch_pencil<kPencilAdjInit>(b));
       }
-      int cur = 0;          // mu buffer receiving mu^{n+1}; the other holds mu^{n+2}
-      bool have_mu2 = false;
       // ---- reverse sweep, one recomputed segment at a time
       for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * K;
@@ -661,28 +656,24 @@ struct Solver final : SolverBase {
         for (int n = s1 - 1; n >= s0; --n) {
           const int j = n - s0;
           PlaneArgs<T> a = plane_args();
-          a.src = bf.mp;                       // partial of mu^{n+1}
-          a.real_out = bf.mu[cur];             // mu^{n+1}
-          a.real_in[0] = have_mu2 ? bf.mu[cur ^ 1] : nullptr;  // mu^{n+2}
+          a.src = bf.mp;                       // partial of c_n mu^{n+1} - mu^{n+2}
           a.real_in[1] = bf.hr + size_t(j) * nr;               // psi^n
-          a.coef = n >= 1 ? 3.0 : 2.0;
           a.dst = bf.gp;                       // partial of g^n
           ADJ_RC(launch_plane<kPlaneAdj>(a));
           PencilArgs<T> b = pencil_args();
           b.src = bf.gp;
           b.w = bf.lam;                        // lambdahat^{n+1} -> lambdahat^n
           b.spec_a = bf.hs + size_t(j) * fe;   // psihat^n
-          b.spec_b = bf.hs + size_t(j + 1) * fe;
-          b.dst = bf.mp;                       // partial of mu^n
+          b.spec_b = n == nsteps - 1 ? bf.hs + size_t(j + 1) * fe : nullptr;  // psihat^T, once
+          b.coef = n >= 1 ? (n - 1 >= 1 ? 3.0 : 2.0) : 0.0;
+          b.dst = bf.mp;                       // partial of c_{n-1} mu^n - mu^{n+1}
           b.red = bf.red;
           ADJ_RC(launch_pencil<kPencilAdj>(b));
-          adj_accumulate_kernel<<<p.batch, 256, 0, stream>>>(bf.red, QC::TILES, bf.acc);
-          ADJ_CUDA(cudaGetLastError());
-          launches += 1;
-          cur ^= 1;
-          have_mu2 = true;
         }
       }
+      adj_reduce_kernel<<<p.batch, 256, 0, stream>>>(bf.red, QC::TILES, bf.acc);
+      ADJ_CUDA(cudaGetLastError());
+      launches += 1;
       // ---- lambda^0 = dL/dpsi^0 in real space
       {
         PencilArgs<T> b = pencil_args();

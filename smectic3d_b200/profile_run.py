@@ -2,7 +2,8 @@
 
     python -m smectic3d_b200.profile_run --boundary neumann --precision fp32 --n 256 --steps 4
 
-It sets a seeded U(-0.1, 0.1) field, takes ``--steps`` steps and exits. The
+It sets a seeded U(-0.1, 0.1) field, takes ``--steps`` steps (or runs the
+adjoint over ``--adjoint`` steps) and exits. The
 kernel order per step is pencil (x) then plane (y,z), after one init plane and
 one init pencil launch. ``ncu -k regex:plane_kernel -s 2 -c 1`` therefore
 captures the plane pass of the second step.
@@ -10,6 +11,8 @@ captures the plane pass of the second step.
 from __future__ import annotations
 
 import argparse
+
+import numpy as np
 
 from .ic import noise
 from .solver import Params, Solver
@@ -24,14 +27,20 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--advection", action="store_true")
+    ap.add_argument("--adjoint", type=int, default=0, metavar="T",
+                    help="instead of plain steps, run sh_adjoint over T steps (checkpoints every 50)")
     args = ap.parse_args(argv)
     p = Params(n=args.n, batch=args.batch, boundary=args.boundary, precision=args.precision, variant=args.variant,
                advection=args.advection)
     with Solver(p) as s:
-        import numpy as np
         psi = np.stack([noise(args.n, r) for r in range(args.batch)]) if args.batch > 1 else noise(args.n, 0)
         s.set_psi(psi)
-        s.step(args.steps)
+        if args.adjoint:
+            lam = np.zeros_like(psi)
+            lam[..., 0] = 1.0
+            s.adjoint(psi, args.adjoint, lam, ckpt_every=50)
+        else:
+            s.step(args.steps)
         s.synchronize()
     print("ok")
 
