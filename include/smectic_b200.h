@@ -109,9 +109,15 @@ int sh_energy_trace(sh_handle* h, double* out, int max_steps, int* count);
  * and how many evaluations happened so far. */
 int sh_l1(sh_handle* h, double* out, int* count);
 
-/* surfTrack pass (periodicFFT/surfTrack.cpp:602-626, 767-806): takes one step
- * and scans every (i, j) column of the new psi for its first crossing.  Writes
- * N*N values per replica: z index (or -1), v_n, H, K (NaN where no crossing). */
+/* Surface pass, one step.  Writes N*N values per replica in (i, j) order:
+ * z index (or -1), v_n, H, K (NaN where no crossing).
+ * Periodic, advected handles: surfTrack (periodicFFT/surfTrack.cpp:602-626,
+ *   767-806): takes one step and scans every column of the new psi (+z, first
+ *   psi < 0 after psi > 0.1).
+ * Neumann handles: the curvature pass of cosFFT/comet/cosNoAdvMorphCurv.cpp:
+ *   742-965 at the current state (spectral psi_xx, psi_yy, psi_zz and d_t psi,
+ *   difference gradients, -z scan for the first psi < 0 after psi > 0.7,
+ *   Megrabov's H and K), then takes one step. */
 int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kgauss);
 
 /* Discrete adjoint of the CNAB2 loop (plain periodic step, SH_CNAB2, no

@@ -374,6 +374,91 @@ class NeumannOracle:
         return self.psi
 
 
+def _fd_wall(a, axis, h):
+    """Centred difference along ``axis`` with the one-sided walls of the
+    Neumann curvature pass: (a[i+1] - a[i-1]) / 2h inside, 2 (a[1] - a[0]) / 2h
+    and 2 (a[-1] - a[-2]) / 2h at the walls (cosNoAdvMorphCurv.cpp:811-872)."""
+    a = np.moveaxis(a, axis, 0)
+    g = np.empty_like(a)
+    g[1:-1] = (a[2:] - a[:-2]) / (2 * h)
+    g[0] = 2 * (a[1] - a[0]) / (2 * h)
+    g[-1] = 2 * (a[-1] - a[-2]) / (2 * h)
+    return np.moveaxis(g, 0, axis)
+
+
+def neumann_curvature_fields(orc: "NeumannOracle"):
+    """Spectral fields of the curvature pass at the oracle's current psi
+    (cosFFT/comet/cosNoAdvMorphCurv.cpp:742-770): psi_xx, psi_yy, psi_zz as
+    REDFT01 of -scale q_a^2 psihat, d_t psi = REDFT01 of scale (aLin psihat + Nhat)."""
+    psi = orc.psi
+    psiq = dct3d(psi)
+    nq = dct3d(orc._nonlin_local(psi))
+    s = orc.scale
+    return {"dxx": idct3d(-s * orc.qx ** 2 * psiq), "dyy": idct3d(-s * orc.qy ** 2 * psiq),
+            "dzz": idct3d(-s * orc.qz ** 2 * psiq), "dt": idct3d(s * (orc.a_lin * psiq + nq))}
+
+
+def neumann_curvature_scan(psi, f, dx: float, threshold: float = 0.7):
+    """Column scan of the Neumann curvature pass (cosNoAdvMorphCurv.cpp:874-965).
+
+    For each (i, j) scan -z from the top for the first psi < 0 after
+    psi > threshold; move up one voxel (k2 = k + 1) when that one is closer to
+    zero.  At k2: |grad psi| from wall-one-sided centred differences, v_n =
+    d_t psi / |grad psi|, mixed derivatives as differences of the gradient
+    (psi_xy along y at k2; psi_xz, psi_yz along z, formula chosen by k as the
+    reference does), and Megrabov's H (/|grad psi|^3) and K (/|grad psi|^4).
+    The x gradient is taken from the current psi (the reference's rank-0 copy
+    of psi can be stale there).  Where the reference's z formula would read
+    past the top of the column (k2 = N-1 with k interior) the one-sided
+    backward formula is used.  Returns z = k2, v_n, H, K (-1 / NaN when no
+    crossing)."""
+    n = psi.shape[0]
+    gx, gy = _fd_wall(psi, 0, dx), _fd_wall(psi, 1, dx)
+    gz = _fd_wall(psi, 2, dx)
+    td = 2 * dx
+    z = -np.ones((n, n), dtype=np.int64)
+    vn = np.full((n, n), np.nan)
+    hh = np.full((n, n), np.nan)
+    kk = np.full((n, n), np.nan)
+    for i in range(n):
+        for j in range(n):
+            col = psi[i, j]
+            track = 0
+            for k in range(n - 1, -1, -1):
+                if col[k] > threshold and track == 0:
+                    track = 1
+                if col[k] < 0 and track == 1:
+                    k2 = k + 1 if abs(col[k]) > abs(col[k + 1]) else k
+                    Gx, Gy, Gz = gx[i, j, k2], gy[i, j, k2], gz[i, j, k2]
+                    g = np.sqrt(Gx * Gx + Gy * Gy + Gz * Gz)
+                    if 0 < j < n - 1:
+                        dxy = (gx[i, j + 1, k2] - gx[i, j - 1, k2]) / td
+                    elif j == 0:
+                        dxy = 2 * (gx[i, 1, k2] - gx[i, 0, k2]) / td
+                    else:
+                        dxy = 2 * (gx[i, j, k2] - gx[i, j - 1, k2]) / td
+                    if 0 < k < n - 1 and k2 + 1 < n:
+                        dxz = (gx[i, j, k2 + 1] - gx[i, j, k2 - 1]) / td
+                        dyz = (gy[i, j, k2 + 1] - gy[i, j, k2 - 1]) / td
+                    elif k == 0:
+                        dxz = 2 * (gx[i, j, k2 + 1] - gx[i, j, k2]) / td
+                        dyz = 2 * (gy[i, j, k2 + 1] - gy[i, j, k2]) / td
+                    else:
+                        dxz = 2 * (gx[i, j, k2] - gx[i, j, k2 - 1]) / td
+                        dyz = 2 * (gy[i, j, k2] - gy[i, j, k2 - 1]) / td
+                    xx, yy, zz = f["dxx"][i, j, k2], f["dyy"][i, j, k2], f["dzz"][i, j, k2]
+                    z[i, j] = k2
+                    vn[i, j] = f["dt"][i, j, k2] / g
+                    hh[i, j] = ((Gy ** 2 + Gz ** 2) * xx + (Gx ** 2 + Gz ** 2) * yy + (Gx ** 2 + Gy ** 2) * zz
+                                - 2 * (Gx * Gy * dxy + Gx * Gz * dxz + Gy * Gz * dyz)) / g ** 3
+                    kk[i, j] = (Gz ** 2 * (xx * yy - dxy ** 2) + Gx ** 2 * (yy * zz - dyz ** 2)
+                                + Gy ** 2 * (xx * zz - dxz ** 2)
+                                + 2 * (Gy * dxy * (Gz * dxz - Gx * zz) + Gx * dxz * (Gy * dyz - Gz * yy)
+                                       + Gz * dyz * (Gx * dxy - Gy * xx))) / g ** 4
+                    break
+    return z, vn, hh, kk
+
+
 # ---------------------------------------------------------------------------
 # diagnostics
 # ---------------------------------------------------------------------------

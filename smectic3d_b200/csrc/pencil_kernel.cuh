@@ -23,14 +23,21 @@ enum PencilMode : int {
   kPencilStep = 0,
   kPencilInit = 1,
   kPencilEnergy = 2,
-  kPencilStepAdv = 3,  // step that also emits the partials of i q_x psihat and opSH psihat
+  kPencilStepAdv = 3,  // step that also emits extra partials: i q_x psihat and opSH psihat (periodic, advection),
+                       // -q_x^2 psihat (Neumann, substrate penalty)
   kPencilInitAdv = 4,
   kPencilStokes = 5,   // Stokes velocity from the stress (periodicFFT/pf3d.cpp:433-447)
-  kPencilXMul = 6,     // partial P -> partial of i q_x times its spectrum (second x derivative of psi)
+  kPencilXMul = 6,     // partial P -> partial of its spectrum times an x-line multiplier (XMul)
   kPencilSpec = 7,     // partial P -> psihat, pencil-major
   kPencilAdjInit = 8,  // adjoint: partial of lambda^T -> lambdahat^T, mu partial
   kPencilAdj = 9,      // adjoint step: lambdahat^n = A lambdahat^{n+1} + ghat^n, mu partial, parameter gradients
   kPencilAdjOut = 10,  // adjoint: lambdahat -> its x-inverse partial (for lambda^0 in real space)
+};
+// multiplier of kPencilXMul
+enum XMulKind : int {
+  kXIqx = 0,     // i q_x (periodic)
+  kXNegQx2 = 1,  // -q_x^2
+  kXOpSH = 2,    // alpha (|q|^2 - q0^2)^2
 };
 // line sets of shared memory a pencil mode uses (FFT scratch, stash, Stokes components)
 __host__ __device__ constexpr int pencil_sets(int mode) {
@@ -76,6 +83,7 @@ struct PencilArgs {
   double* red;          // per-CTA spectral energy partial [rep][grid.x]
   int* nonfinite;       // set to 1 when a new coefficient is NaN/Inf
   double coef;          // adjoint: c_{n-1} of the emitted mu combination (0 on the last reverse step)
+  int xmul;             // kPencilXMul: XMulKind
   const T* q;           // wavenumber table (N entries)
   const cplx<T>* tw;    // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
@@ -431,15 +439,25 @@ pencil_kernel(PencilArgs<T> a) {
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
     Ops::forward(v, L, t, tw);
-    // P is x-inverse of (scale X); forward x gives N scale X: multiply by i q_x / N
-    const T invn = T(1) / T(N);
+    // P is the x-inverse of (scale X); its forward x transform is N scale X
+    // (2N scale X for REDFT10 after REDFT01): multiply by m(q) / N (/ 2N)
+    const T invn = T(1) / T(DCT ? 2 * N : N);
+    const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha);
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
-        const T qx = __ldg(&a.q[out_index<N, -1>(t, b, r)]) * invn;
+        const T qx = __ldg(&a.q[out_index<N, -1>(t, b, r)]);
         const cplx<T> val = v[b * RL + r];
-        v[b * RL + r] = mk<T>(-qx * val.y, qx * val.x);
+        if (a.xmul == kXIqx) {
+          v[b * RL + r] = mk<T>(-qx * invn * val.y, qx * invn * val.x);
+        } else if (a.xmul == kXNegQx2) {
+          v[b * RL + r] = cscale<T>(val, -qx * qx * invn);
+        } else {
+          const T d0 = qx * qx + qy * qy + qz0 * qz0 - q02;
+          const T d1 = DCT ? qx * qx + qy * qy + qz1 * qz1 - q02 : d0;
+          v[b * RL + r] = mk<T>(alpha * d0 * d0 * invn * val.x, alpha * d1 * d1 * invn * val.y);
+        }
       }
   } else if constexpr (MODE == kPencilStokes) {
     if constexpr (!DCT) {
@@ -532,7 +550,34 @@ pencil_kernel(PencilArgs<T> a) {
     __syncthreads();
     Ops::store_tile(buf, a.dst + plane_base, f0);
   } else if constexpr (MODE == kPencilStepAdv || MODE == kPencilInitAdv) {
-    if constexpr (!DCT) {
+    if constexpr (DCT) {
+      // v = scale psihat^{n+1}; emit the partials of v and of -q_x^2 v (the x
+      // half of the substrate's in-plane Laplacian), one inverse x transform each
+      cplx<T>* stash = buf + TK * LS + line * LS;
+      __syncwarp();
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) stash[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
+      __syncwarp();
+      cplx<T>* outs[2] = {a.dst, a.dst_x};
+#pragma unroll 1
+      for (int o = 0; o < 2; ++o) {
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) {
+            const int kx = out_index<N, -1>(t, b, r);
+            const cplx<T> val = stash[pad(kx)];
+            const T qx = __ldg(&a.q[kx]);
+            v[b * RL + r] = o == 0 ? val : cscale<T>(val, -qx * qx);
+          }
+        Ops::inverse_to_line(v, L, t, tw);
+        __syncthreads();
+        Ops::store_tile(buf, outs[o] + plane_base, f0);
+        __syncthreads();
+      }
+    } else {
       // v = scale psihat^{n+1}; emit the partials of v, i q_x v and opSH v
       // (periodicFFT/pf3d.cpp:404-407), one inverse x transform each
       cplx<T>* stash = buf + TK * LS + line * LS;

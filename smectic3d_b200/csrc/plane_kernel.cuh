@@ -28,7 +28,7 @@ namespace shb {
 
 enum PlaneMode : int { kPlaneStep = 0, kPlaneInit = 1, kPlaneGetPsi = 2, kPlaneInvReal = 3, kPlaneFwdReal = 4, kPlaneAdj = 5 };
 // spectral multiplier applied to the partial spectrum as the plane is loaded
-enum SpecMult : int { kMulNone = 0, kMulIqy = 1, kMulIqz = 2, kMulNegQy2 = 3 };
+enum SpecMult : int { kMulNone = 0, kMulIqy = 1, kMulIqz = 2, kMulNegQy2 = 3, kMulNegQz2 = 4 };
 // real-space operation of kPlaneFwdReal
 enum RealOp : int {
   kOpProduct = 0,   // in[0] * in[1]                      (stress S_i = (L psi) d_i psi)
@@ -99,12 +99,21 @@ struct PlaneArgs {
   const cplx<T>* tw;      // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
   int flags;
-  // real-field modes (periodic): wavenumber table, multiplier, real inputs / output
+  // real-field modes: wavenumber table, multiplier, real inputs / output
   const T* q;
   int mult;
   int op;
   const T* real_in[7];
   T* real_out;
+  // kPlaneInvReal: optional second partial, added after its own multiplier
+  const cplx<T>* src2;
+  int mult2;
+  int real_zn;  // > 0: real_out holds only z < real_zn, layout [rep][x][y][real_zn]
+  // Neumann substrate penalty: N += wall[z] * lperp for z < kwall, with lperp
+  // the in-plane Laplacian of psi in layout [rep][x][y][kwall]
+  const T* wall;
+  const T* lperp;
+  int kwall;
 };
 
 // Cluster barrier.  RELEASE orders this thread's earlier shared-memory writes
@@ -203,6 +212,15 @@ struct PlaneOps {
   // ---- column phase, inverse direction ---------------------------------
   // multiply a periodic spectral value at (ky, kz) by i q_y, i q_z or -q_y^2
   static __device__ __forceinline__ cplx<T> apply_mult(cplx<T> v, int mult, const T* q, int ky, int kz) {
+    if (mult == kMulNegQz2) {
+      if constexpr (DCT) {  // the pair holds kz = 2 kz, 2 kz + 1
+        const T qa = __ldg(&q[2 * kz]), qb = __ldg(&q[2 * kz + 1]);
+        return mk<T>(-qa * qa * v.x, -qb * qb * v.y);
+      } else {
+        const T qq = __ldg(&q[kz]);
+        return cscale<T>(v, -qq * qq);
+      }
+    }
     if (mult == kMulIqy || mult == kMulIqz) {
       const T qq = __ldg(&q[mult == kMulIqy ? ky : kz]);
       return mk<T>(-qq * v.y, qq * v.x);
@@ -214,8 +232,11 @@ struct PlaneOps {
     return v;
   }
 
+  // Load this CTA's columns of a partial spectrum (times ``mult``), plus a
+  // second partial ``plane2`` times ``mult2`` when given.
   static __device__ void col_load(cplx<T>* buf, const cplx<T>* __restrict__ plane, int rank, int mult = kMulNone,
-                                  const T* q = nullptr) {
+                                  const T* q = nullptr, const cplx<T>* __restrict__ plane2 = nullptr,
+                                  int mult2 = kMulNone) {
     const int c0 = rank * NC;
     // NC * N == THREADS * E: every thread issues its E loads before any store
     cplx<T> tmp[E];
@@ -231,6 +252,14 @@ struct PlaneOps {
         tmp[e] = apply_mult(tmp[e], mult, q, idx / NC, c0 + idx % NC);
       }
     }
+    if (plane2) {
+#pragma unroll
+      for (int e = 0; e < E; ++e) {
+        const int idx = threadIdx.x + THREADS * e;
+        const cplx<T> u = apply_mult(plane2[(idx / NC) * (N / 2) + c0 + idx % NC], mult2, q, idx / NC, c0 + idx % NC);
+        tmp[e] = cadd<T>(tmp[e], u);
+      }
+    }
     constexpr int KPT = (N + THREADS - 1) / THREADS;  // ky per thread for the kz=0 / N/2 columns
     cplx<T> nyq[KPT];
     if constexpr (!DCT) {
@@ -238,7 +267,10 @@ struct PlaneOps {
 #pragma unroll
         for (int m = 0; m < KPT; ++m) {
           const int ky = threadIdx.x + m * THREADS;
-          if (ky < N) nyq[m] = apply_mult(plane[N * (N / 2) + ky], mult, q, ky, N / 2);
+          if (ky < N) {
+            nyq[m] = apply_mult(plane[N * (N / 2) + ky], mult, q, ky, N / 2);
+            if (plane2) nyq[m] = cadd<T>(nyq[m], apply_mult(plane2[N * (N / 2) + ky], mult2, q, ky, N / 2));
+          }
         }
       }
     }
@@ -577,7 +609,8 @@ struct PlaneOps {
 // on the plane z = N/2, periodicFFT/pf3dMorph.cpp:456-467).  ``v`` holds psi
 // on entry and N(psi) on exit.
 template <typename T, int N, int CL, bool DCT>
-__device__ __forceinline__ void row_nonlin(cplx<T> (&v)[Plan<N>::E], cplx<T>* L, int t, const PointParams& pp) {
+__device__ __forceinline__ void row_nonlin(cplx<T> (&v)[Plan<N>::E], cplx<T>* L, int t, const PointParams& pp,
+                                           const T* wall = nullptr, const T* lp0 = nullptr, int kwall = 0) {
   using Ops = PlaneOps<T, N, CL, DCT>;
   constexpr int E = Plan<N>::E;
   constexpr int RL = PlaneCfg<T, N, CL, DCT>::RL_INV;
@@ -602,6 +635,11 @@ __device__ __forceinline__ void row_nonlin(cplx<T> (&v)[Plan<N>::E], cplx<T>* L,
         const T c = T(2.0 * pp.w_mid * pp.inv_dz2);
         o.x += c * (lo.x - T(2) * p.x + hi.x);
         o.y += c * (lo.y - T(2) * p.y + hi.y);
+      }
+      if (z < kwall) {  // substrate penalty (cosFFT/comet/cosNoAdvMorph.cpp:591-623)
+        const T w = wall[z];
+        o.x += w * lp0[z];
+        o.y += w * lp0[kwall + z];
       }
       v[b * RL + r] = o;
     }
@@ -649,7 +687,7 @@ plane_kernel(PlaneArgs<T> a) {
 
   if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi || MODE == kPlaneInvReal || MODE == kPlaneAdj) {
     if constexpr (MODE == kPlaneInvReal) {
-      Ops::col_load(buf, a.src + plane_off, rank, a.mult, a.q);
+      Ops::col_load(buf, a.src + plane_off, rank, a.mult, a.q, a.src2 ? a.src2 + plane_off : nullptr, a.mult2);
     } else {
       Ops::col_load(buf, a.src + plane_off, rank);
     }
@@ -691,7 +729,21 @@ plane_kernel(PlaneArgs<T> a) {
         }
       }
     }
-    if (MODE == kPlaneInvReal || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
+    if (MODE == kPlaneInvReal && a.real_zn > 0) {
+      // only the planes z < real_zn, compact
+      const int zn = a.real_zn;
+      T* o0 = a.real_out + ((size_t(rep) * N + x) * N + y0) * zn;
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int z = Ops::row_z(t, b, r);
+          if (z < zn) {
+            o0[z] = v[b * RL + r].x;
+            o0[zn + z] = v[b * RL + r].y;
+          }
+        }
+    } else if (MODE == kPlaneInvReal || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -719,7 +771,8 @@ plane_kernel(PlaneArgs<T> a) {
       Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
     }
     if constexpr (MODE == kPlaneStep) {
-      row_nonlin<T, N, CL, DCT>(v, L, t, a.pp);
+      const T* lp0 = a.kwall > 0 ? a.lperp + ((size_t(rep) * N + x) * N + y0) * a.kwall : nullptr;
+      row_nonlin<T, N, CL, DCT>(v, L, t, a.pp, a.wall, lp0, a.kwall);
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
     }
@@ -778,6 +831,11 @@ plane_kernel(PlaneArgs<T> a) {
               const T c = T(2.0 * a.pp.w_mid * a.pp.inv_dz2);
               na += c * (T(src[size_t(y0) * N + z - 1]) - T(2) * pa + T(src[size_t(y0) * N + z + 1]));
               nb += c * (T(src[size_t(y0 + 1) * N + z - 1]) - T(2) * pb + T(src[size_t(y0 + 1) * N + z + 1]));
+            }
+            if (z < a.kwall) {  // substrate penalty of psi^0
+              const T* lp0 = a.lperp + ((size_t(rep) * N + x) * N + y0) * a.kwall;
+              na += a.wall[z] * lp0[z];
+              nb += a.wall[z] * lp0[a.kwall + z];
             }
             pa = na;
             pb = nb;

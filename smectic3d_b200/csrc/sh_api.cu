@@ -155,7 +155,10 @@ int sh_create(const sh_params* p, sh_handle** out) {
   if (p->l1_interval < 0) return fail(nullptr, SH_EINVAL, "l1_interval must be >= 0");
   if (p->advection && p->boundary != SH_PERIODIC)
     return fail(nullptr, SH_EINVAL, "advection is defined for the periodic boundary only");
-  if (p->sub_sigma != 0.0) return fail(nullptr, SH_EUNSUPPORTED, "substrate penalty is not built into this library version");
+  if (p->sub_sigma != 0.0) {
+    if (p->boundary != SH_NEUMANN) return fail(nullptr, SH_EUNSUPPORTED, "the substrate penalty is defined for the Neumann boundary");
+    if (!(p->sub_z0 > 0.0)) return fail(nullptr, SH_EINVAL, "sub_z0 must be > 0");
+  }
   if (p->variant < 0) return fail(nullptr, SH_EINVAL, "variant must be >= 0");
 
   SolverBase* s = nullptr;

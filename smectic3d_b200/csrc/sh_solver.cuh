@@ -109,6 +109,16 @@ struct Solver final : SolverBase {
   T* SR[4] = {};     // surface pass: psi_xx, psi_yy, psi_xy, H-numerator (allocated on first use)
   int* d_zout = nullptr;
   double* d_surf[3] = {nullptr, nullptr, nullptr};
+  // Neumann substrate penalty (sub_sigma != 0): partial of -q_x^2 scale psihat,
+  // the in-plane Laplacian of psi on the planes z < kwall ([rep][x][y][kwall])
+  // and wall(z) on those planes
+  cplx<T>* Pxx = nullptr;
+  T* Lp = nullptr;
+  T* d_wall = nullptr;
+  int kwall = 0;
+  // Neumann curvature pass: psi, psi_xx, psi_yy, psi_zz, L psi and a scratch partial
+  T* CR[5] = {};
+  cplx<T>* Psc = nullptr;
   bool real_fields_current = false;
   // adjoint work buffers, kept for the handle's lifetime once allocated
   struct AdjBufs {
@@ -146,6 +156,11 @@ struct Solver final : SolverBase {
     for (auto* r : SR) cudaFree(r);
     cudaFree(d_zout);
     for (auto* d : d_surf) cudaFree(d);
+    cudaFree(Pxx);
+    cudaFree(Lp);
+    cudaFree(d_wall);
+    for (auto* r : CR) cudaFree(r);
+    cudaFree(Psc);
   }
 
   size_t field_elems() const { return size_t(p.batch) * N * FP; }
@@ -193,6 +208,26 @@ struct Solver final : SolverBase {
         SHB_CUDA(cudaMalloc(&PSH, fe * sizeof(cplx<T>)));
         for (auto& p3 : S3) SHB_CUDA(cudaMalloc(&p3, fe * sizeof(cplx<T>)));
         for (auto& r : R) SHB_CUDA(cudaMalloc(&r, size_t(p.batch) * N * N * N * sizeof(T)));
+      }
+    }
+    if (p.sub_sigma != 0.0) {
+      if constexpr (!DCT) {
+        err = "the substrate penalty is defined for the Neumann boundary only";
+        return SH_EINVAL;
+      } else {
+        // wall(z) = sigma exp(-z / z0) (cosFFT/comet/cosNoAdvMorph.cpp:67-74), kept on the planes
+        // where it is at least 1e-30 |sigma|; below that its term is under the FP64 rounding of N
+        std::vector<T> hw;
+        for (int k = 0; k < N; ++k) {
+          const double w = p.sub_sigma * std::exp(-double(k) / p.sub_z0);
+          if (std::fabs(w) < 1e-30 * std::fabs(p.sub_sigma)) break;
+          hw.push_back(T(w));
+        }
+        kwall = int(hw.size());
+        SHB_CUDA(cudaMalloc(&Pxx, fe * sizeof(cplx<T>)));
+        SHB_CUDA(cudaMalloc(&Lp, size_t(p.batch) * N * N * kwall * sizeof(T)));
+        SHB_CUDA(cudaMalloc(&d_wall, kwall * sizeof(T)));
+        SHB_CUDA(cudaMemcpy(d_wall, hw.data(), kwall * sizeof(T), cudaMemcpyHostToDevice));
       }
     }
     SHB_CUDA(cudaMalloc(&tw, tw_total<N>() * sizeof(cplx<T>)));
@@ -289,26 +324,61 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
+  // In-plane Laplacian of the current psi on the substrate planes:
+  // Lp = IDCT_yz(partial of -q_x^2 scale psihat  -  q_y^2 x partial of scale psihat)
+  int substrate_lperp() {
+    PlaneArgs<T> a = plane_args();
+    a.src = Pxx;
+    a.src2 = P;
+    a.mult2 = kMulNegQy2;
+    a.real_out = Lp;
+    a.real_zn = kwall;
+    return launch_plane<kPlaneInvReal>(a);
+  }
+  PlaneArgs<T> plane_args_step() const {
+    PlaneArgs<T> a = plane_args();
+    a.wall = d_wall;
+    a.lperp = Lp;
+    a.kwall = kwall;
+    return a;
+  }
+
   int init_from_psi() override {
     int rc;
     PlaneArgs<T> a = plane_args();
     a.psi_in = d_psi;
     a.dst2 = P;   // partial of psi^0 (consumed by the init pencil, then overwritten)
     a.dst = Nt;   // partial of N(psi^0): the first Nhat (Euler start)
-    if ((rc = launch_plane<kPlaneInit>(a))) return rc;
     PencilArgs<T> b = pencil_args();
     b.src = P;
     b.src2 = Nt;
     b.w = W;
     b.dst = P;
-    if (p.advection) {
-      b.dst_x = Px;
-      b.dst_sh = PSH;
+    if (kwall > 0) {
+      // N(psi^0) carries the substrate term of psi^0 (cosFFT/comet/cosNoAdvMorph.cpp:486-529):
+      // a first pass yields psi^0's partials, hence its in-plane Laplacian; the second
+      // pass builds N-hat^{-1} and W^0 with it
+      if ((rc = launch_plane<kPlaneInit>(a))) return rc;
+      b.dst_x = Pxx;
       if ((rc = launch_pencil<kPencilInitAdv>(b))) return rc;
-      // the first advected N (N-hat^{-1} above discards advection, pf3d.cpp:363-374)
-      if ((rc = adv_nonlinear(0))) return rc;
+      if ((rc = substrate_lperp())) return rc;
+      a = plane_args_step();
+      a.psi_in = d_psi;
+      a.dst2 = P;
+      a.dst = Nt;
+      if ((rc = launch_plane<kPlaneInit>(a))) return rc;
+      if ((rc = launch_pencil<kPencilInitAdv>(b))) return rc;
     } else {
-      if ((rc = launch_pencil<kPencilInit>(b))) return rc;
+      if ((rc = launch_plane<kPlaneInit>(a))) return rc;
+      if (p.advection) {
+        b.dst_x = Px;
+        b.dst_sh = PSH;
+        if ((rc = launch_pencil<kPencilInitAdv>(b))) return rc;
+        // the first advected N (N-hat^{-1} above discards advection, pf3d.cpp:363-374)
+        if ((rc = adv_nonlinear(0))) return rc;
+      } else {
+        if ((rc = launch_pencil<kPencilInit>(b))) return rc;
+      }
     }
     if (p.l1_interval > 0)
       SHB_CUDA(cudaMemcpyAsync(d_stash, d_psi, size_t(p.batch) * n3() * sizeof(double), cudaMemcpyDeviceToDevice,
@@ -385,9 +455,16 @@ struct Solver final : SolverBase {
         if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
         if ((rc = adv_nonlinear(diag))) return rc;
       } else {
-        if ((rc = launch_pencil<kPencilStep>(b))) return rc;
-        if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
-        PlaneArgs<T> a = plane_args();
+        if (kwall > 0) {  // Neumann substrate: also the -q_x^2 partial, then the in-plane Laplacian
+          b.dst_x = Pxx;
+          if ((rc = launch_pencil<kPencilStepAdv>(b))) return rc;
+          if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
+          if ((rc = substrate_lperp())) return rc;
+        } else {
+          if ((rc = launch_pencil<kPencilStep>(b))) return rc;
+          if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
+        }
+        PlaneArgs<T> a = plane_args_step();
         a.src = P;
         a.dst = Nt;
         a.flags = diag;
@@ -707,8 +784,64 @@ struct Solver final : SolverBase {
   // fields of state n.
   int surface_step(int* z, double* vn, double* hh, double* kk) override {
     if constexpr (DCT) {
-      err = "surface tracking is defined for the periodic boundary";
-      return SH_EINVAL;
+      // curvature pass of cosFFT/comet/cosNoAdvMorphCurv.cpp:742-965 at state n, then one step
+      int rc;
+      const size_t nr = size_t(p.batch) * N * N * N, nc = size_t(p.batch) * N * N;
+      if (!CR[0]) {
+        for (auto& r : CR) SHB_CUDA(cudaMalloc(&r, nr * sizeof(T)));
+        SHB_CUDA(cudaMalloc(&Psc, field_elems() * sizeof(cplx<T>)));
+        SHB_CUDA(cudaMalloc(&d_zout, nc * sizeof(int)));
+        for (auto& d : d_surf) SHB_CUDA(cudaMalloc(&d, nc * sizeof(double)));
+      }
+      // psi, psi_yy, psi_zz from the partial of psi; psi_xx and L psi through an x multiplier
+      const int mult[3] = {kMulNone, kMulNegQy2, kMulNegQz2};
+      T* outs[3] = {CR[0], CR[2], CR[3]};
+      for (int i = 0; i < 3; ++i) {
+        PlaneArgs<T> a = plane_args();
+        a.src = P;
+        a.mult = mult[i];
+        a.real_out = outs[i];
+        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      }
+      const int xm[2] = {kXNegQx2, kXOpSH};
+      T* xo[2] = {CR[1], CR[4]};
+      for (int i = 0; i < 2; ++i) {
+        PencilArgs<T> b = pencil_args();
+        b.src = P;
+        b.dst = Psc;
+        b.xmul = xm[i];
+        if ((rc = launch_pencil<kPencilXMul>(b))) return rc;
+        PlaneArgs<T> a = plane_args();
+        a.src = Psc;
+        a.real_out = xo[i];
+        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      }
+      CurvArgs<T> ca;
+      ca.psi = CR[0];
+      ca.dxx = CR[1];
+      ca.dyy = CR[2];
+      ca.dzz = CR[3];
+      ca.lpsi = CR[4];
+      ca.wall = d_wall;
+      ca.lperp = Lp;
+      ca.kwall = kwall;
+      ca.pp = point_params();
+      ca.n = N;
+      ca.dx = p.dx;
+      ca.zout = d_zout;
+      ca.vn = d_surf[0];
+      ca.hh = d_surf[1];
+      ca.kk = d_surf[2];
+      curv_scan_kernel<T><<<dim3((N * N + 127) / 128, p.batch), 128, 0, stream>>>(ca);
+      SHB_CUDA(cudaGetLastError());
+      ++launches;
+      if ((rc = step_async(1))) return rc;
+      SHB_CUDA(cudaMemcpyAsync(z, d_zout, nc * sizeof(int), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(vn, d_surf[0], nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(hh, d_surf[1], nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaMemcpyAsync(kk, d_surf[2], nc * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaStreamSynchronize(stream));
+      return SH_OK;
     } else {
       if (!p.advection) {
         err = "surface tracking runs the advected step (advection = 1)";

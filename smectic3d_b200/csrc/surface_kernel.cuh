@@ -1,4 +1,6 @@
-// surfTrack surface pass (periodicFFT/surfTrack.cpp:592-626, 744-806).
+// Surface passes.
+//
+// surfTrack (periodic; periodicFFT/surfTrack.cpp:592-626, 744-806):
 //
 // surface_prep (elementwise, state n): from psi, grad psi, L psi, u and the
 // second derivatives psi_xx, psi_yy, psi_xy (all real fields) it forms
@@ -8,6 +10,14 @@
 // surface_scan (one thread per (x, y) column, state n+1): the first psi < 0
 // after psi > 0.1 scanning +z, stepping back one voxel when that one is closer
 // to zero; outputs the unadjusted z index (the reference writes k), v_n, H, K.
+//
+// Neumann curvature pass (cosFFT/comet/cosNoAdvMorphCurv.cpp:742-965):
+// curv_scan, one thread per (x, y) column at state n, scanning -z from the top
+// for the first psi < 0 after psi > 0.7 and moving up one voxel when that one
+// is closer to zero; at that voxel the gradient is taken by centred
+// differences (one-sided at the walls), the mixed derivatives as differences
+// of the gradient, psi_xx, psi_yy, psi_zz and L psi come from the spectral
+// fields, d_t psi = eps psi - L psi + N(psi), and Megrabov's H and K follow.
 #pragma once
 #include "sh_common.cuh"
 
@@ -85,6 +95,109 @@ __global__ void surface_scan_kernel(const T* __restrict__ psi_new, const T* __re
   vn[o] = double(dtpsi[idx]) / g;
   hh[o] = double(hnum[idx]) / g;
   kk[o] = double(knum[idx]) / (g * g);
+}
+
+template <typename T>
+struct CurvArgs {
+  const T* psi;    // state n, [rep][x][y][z]
+  const T* dxx;    // psi_xx, psi_yy, psi_zz (spectral)
+  const T* dyy;
+  const T* dzz;
+  const T* lpsi;   // L psi = opSH psi
+  const T* wall;   // substrate term of N, planes z < kwall (optional)
+  const T* lperp;
+  int kwall;
+  PointParams pp;
+  int n;
+  double dx;
+  int* zout;
+  double* vn;
+  double* hh;
+  double* kk;
+};
+
+// centred difference along one axis (stride s, index i of n), one-sided at the walls
+template <typename T>
+__device__ __forceinline__ double curv_grad(const T* f, size_t at, size_t s, int i, int n, double td) {
+  if (i > 0 && i < n - 1) return (double(f[at + s]) - double(f[at - s])) / td;
+  if (i == 0) return 2.0 * (double(f[at + s]) - double(f[at])) / td;
+  return 2.0 * (double(f[at]) - double(f[at - s])) / td;
+}
+
+template <typename T>
+__global__ void curv_scan_kernel(CurvArgs<T> a) {
+  const int rep = blockIdx.y;
+  const int n = a.n;
+  const long long col = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (col >= (long long)n * n) return;
+  const int i = int(col / n), j = int(col % n);
+  const size_t sx = size_t(n) * n, sy = size_t(n);
+  const size_t base = size_t(rep) * n * sx + size_t(col) * n;  // (rep, i, j, 0)
+  const size_t o = size_t(rep) * n * n + col;
+  const T* psi = a.psi;
+  int k2 = -1, kf = -1;
+  int track = 0;
+  for (int k = n - 1; k >= 0; --k) {
+    const T v = psi[base + k];
+    if (v > T(0.7) && track == 0) track = 1;
+    if (v < T(0) && track == 1) {
+      kf = k;
+      k2 = fabs(double(v)) > fabs(double(psi[base + k + 1])) ? k + 1 : k;
+      break;
+    }
+  }
+  a.zout[o] = k2;
+  if (k2 < 0) {
+    a.vn[o] = a.hh[o] = a.kk[o] = nan("");
+    return;
+  }
+  const double td = 2.0 * a.dx;
+  const size_t at = base + k2;
+  const double gx = curv_grad(psi, at, sx, i, n, td);
+  const double gy = curv_grad(psi, at, sy, j, n, td);
+  const double gz = curv_grad(psi, at, 1, k2, n, td);
+  const double g = sqrt(gx * gx + gy * gy + gz * gz);
+  // psi_xy: y difference of the x gradient at k2
+  double dxy;
+  {
+    const int jp = j < n - 1 ? j + 1 : j, jm = j > 0 ? j - 1 : j;
+    const double gp = curv_grad(psi, at + (size_t(jp) - j) * sy, sx, i, n, td);
+    const double gm = curv_grad(psi, at - (size_t(j) - jm) * sy, sx, i, n, td);
+    dxy = (j > 0 && j < n - 1) ? (gp - gm) / td : 2.0 * (gp - gm) / td;
+  }
+  // psi_xz, psi_yz: z differences of the x and y gradients; the formula follows
+  // the scan index k, as the reference does, and the top of the column is one-sided
+  double dxz, dyz;
+  {
+    int zp, zm;
+    if (kf > 0 && kf < n - 1 && k2 + 1 < n) {
+      zp = k2 + 1;
+      zm = k2 - 1;
+    } else if (kf == 0) {
+      zp = k2 + 1;
+      zm = k2;
+    } else {
+      zp = k2;
+      zm = k2 - 1;
+    }
+    const double c = (zp - zm == 2) ? 1.0 : 2.0;
+    dxz = c * (curv_grad(psi, base + zp, sx, i, n, td) - curv_grad(psi, base + zm, sx, i, n, td)) / td;
+    dyz = c * (curv_grad(psi, base + zp, sy, j, n, td) - curv_grad(psi, base + zm, sy, j, n, td)) / td;
+  }
+  const double xx = a.dxx[at], yy = a.dyy[at], zz = a.dzz[at];
+  const double p = psi[at];
+  double nl = double(nonlin_eval<double>(p, a.pp.beta, a.pp.gamma, a.pp.nonlin));
+  if (a.pp.w_mid != 0.0 && k2 == n / 2)
+    nl += 2.0 * a.pp.w_mid * a.pp.inv_dz2 * (double(psi[at - 1]) - 2.0 * p + double(psi[at + 1]));
+  if (k2 < a.kwall) nl += double(a.wall[k2]) * double(a.lperp[(size_t(rep) * sx + col) * a.kwall + k2]);
+  const double dt_psi = a.pp.eps[rep] * p - double(a.lpsi[at]) + nl;
+  a.vn[o] = dt_psi / g;
+  a.hh[o] = ((gy * gy + gz * gz) * xx + (gx * gx + gz * gz) * yy + (gx * gx + gy * gy) * zz -
+             2.0 * (gx * gy * dxy + gx * gz * dxz + gy * gz * dyz)) /
+            (g * g * g);
+  a.kk[o] = (gz * gz * (xx * yy - dxy * dxy) + gx * gx * (yy * zz - dyz * dyz) + gy * gy * (xx * zz - dxz * dxz) +
+             2.0 * (gy * dxy * (gz * dxz - gx * zz) + gx * dxz * (gy * dyz - gz * yy) + gz * dyz * (gx * dxy - gy * xx))) /
+            (g * g * g * g);
 }
 
 }  // namespace shb

@@ -183,8 +183,10 @@ class Solver:
         return out, cnt.value
 
     def surface_step(self):
-        """surfTrack pass: one advected step; per (x, y) column of the new psi the
-        first crossing z (-1 if none), v_n, H and K (NaN if none)."""
+        """Surface pass and one step; per (x, y) column the crossing z (-1 if
+        none), v_n, H and K (NaN if none).  Periodic advected handles run
+        surfTrack on the new psi; Neumann handles run the curvature pass
+        (Megrabov H and K) on the psi before the step."""
         n, b = self.params.n, self.params.batch
         shape = (b, n, n) if b > 1 else (n, n)
         z = np.empty(shape, dtype=np.int32)

@@ -101,6 +101,17 @@ def periodic_advected():
     return _pack(p, psi0=psi0, psi=o.psi, steps=10, advect=True, energy=O.energy_spectral_periodic(o.psi, p))
 
 
+def neumann_substrate():
+    # substrate penalty sigma exp(-z/z0) * in-plane Laplacian on the bottom planes
+    # (cosFFT/comet/cosNoAdvMorph.cpp:67-74, 591-623)
+    n = 16
+    p = O.Params(n=n, dt=0.05, sub_sigma=0.5, sub_z0=1.5)
+    psi0 = ic.cos_bottom_hyperboloid(n, p.dx) + ic.noise(n, 8, 0.05)
+    o = O.NeumannOracle(psi0, p)
+    o.run(10)
+    return _pack(p, psi0=psi0, psi=o.psi, steps=10)
+
+
 CASES = {
     "periodic_plain_16": periodic_plain,
     "periodic_lamellae_32": periodic_lamellae_ref_ic,
@@ -109,6 +120,7 @@ CASES = {
     "neumann_hyperboloid_16": neumann_hyperboloid,
     "neumann_l1_32": neumann_l1,
     "periodic_advected_16": periodic_advected,
+    "neumann_substrate_16": neumann_substrate,
 }
 
 

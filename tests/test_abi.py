@@ -97,6 +97,20 @@ def test_create_rejects_neumann_advection(lib):
     assert lib.sh_create(C.byref(p), C.byref(h)) == L.SH_EINVAL
 
 
+@pytest.mark.parametrize("boundary,z0,code", [(L.SH_PERIODIC, 1e-4, L.SH_EUNSUPPORTED), (L.SH_NEUMANN, 0.0, L.SH_EINVAL),
+                                                (L.SH_NEUMANN, -1.0, L.SH_EINVAL)])
+def test_create_rejects_bad_substrate(lib, boundary, z0, code):
+    # the substrate penalty (cosFFT/comet/cosNoAdvMorph.cpp:67-74) is a Neumann feature with z0 > 0
+    p = L.ShParams()
+    lib.sh_default_params(C.byref(p))
+    p.boundary = boundary
+    p.sub_sigma = 0.5
+    p.sub_z0 = z0
+    h = C.c_void_p()
+    assert lib.sh_create(C.byref(p), C.byref(h)) == code
+    assert not h.value
+
+
 def test_null_arguments(lib):
     assert lib.sh_create(None, None) == L.SH_EINVAL
     assert lib.sh_destroy(None) == L.SH_EINVAL

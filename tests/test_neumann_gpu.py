@@ -1,0 +1,104 @@
+"""GPU parity of the Neumann-only parts of the path against the FP64 oracle:
+the substrate penalty (cosFFT/comet/cosNoAdvMorph.cpp:67-74, 591-623) and the
+curvature pass (cosFFT/comet/cosNoAdvMorphCurv.cpp:742-965)."""
+import math
+
+import numpy as np
+import pytest
+
+import smectic3d_b200 as S
+from oracle import sh_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "fp32": 1e-5}
+
+
+def rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def oracle_params(p: S.Params) -> O.Params:
+    return O.Params(n=p.n, dx=p.dx, dt=p.dt, eps=p.eps, beta=p.beta, gamma=p.gamma, alpha=p.alpha, q0=p.q0,
+                    nonlinearity=p.nonlinearity, scheme=p.scheme, w_mid=p.w_mid, sub_sigma=p.sub_sigma,
+                    sub_z0=p.sub_z0)
+
+
+def undulated(n, dx, amp=0.9, phase=0.37):
+    """Lamellae along z displaced by a Neumann-compatible height field, with
+    off-grid phases so that no grid value of psi is exactly 0 or 0.7."""
+    c = np.arange(n) * dx
+    L = n * dx
+    h = amp * (np.cos(2 * np.pi * c / L + 0.3)[:, None, None] * np.cos(np.pi * c / L + 0.2)[None, :, None])
+    return 1.3 * np.cos(c[None, None, :] - h - phase)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("z0", [1e-4, 2.0])
+@pytest.mark.parametrize("n", [32, 64])
+def test_substrate_matches_oracle(n, z0, prec):
+    """wall(z) = sigma exp(-z/z0) times the in-plane Laplacian of psi^n joins N;
+    z0 = 1e-4 (the reference's value) leaves only the bottom plane, 2.0 a
+    band of planes."""
+    p = S.Params(n=n, boundary="neumann", precision=prec, dt=0.05, eps=-0.7, sub_sigma=0.5, sub_z0=z0)
+    psi0 = S.ic.cos_bottom_hyperboloid(n, p.dx) + S.ic.noise(n, 3, 0.05)
+    orc = O.NeumannOracle(psi0, oracle_params(p))
+    orc.run(40)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(40)
+        psi = s.get_psi()
+    assert rel(psi, orc.psi) <= TOL[prec]
+    # and the term matters: without it the state differs far beyond the tolerance
+    q = O.NeumannOracle(psi0, oracle_params(S.Params(n=n, boundary="neumann", dt=0.05, eps=-0.7)))
+    q.run(40)
+    assert rel(q.psi, orc.psi) > 1e3 * TOL["fp64"]
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [32, 64])
+def test_curvature_pass_matches_oracle(n, prec):
+    p = S.Params(n=n, boundary="neumann", precision=prec, dt=0.05, eps=-0.7)
+    psi0 = undulated(n, p.dx)
+    orc = O.NeumannOracle(psi0, oracle_params(p))
+    orc.run(3)
+    f = O.neumann_curvature_fields(orc)
+    zo, vo, ho, ko = O.neumann_curvature_scan(orc.psi, f, p.dx)
+    orc.step()
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(3)
+        z, vn, hh, kk = s.surface_step()
+        assert rel(s.get_psi(), orc.psi) <= TOL[prec]  # the pass also took the step
+    found = zo >= 0
+    assert found.mean() > 0.9
+    same = z == zo
+    assert same.mean() >= (1.0 if prec == "fp64" else 0.99)
+    m = same & found
+    tol = 1e-8 if prec == "fp64" else 2e-3
+    for got, ref in ((vn, vo), (hh, ho), (kk, ko)):
+        scale = max(np.abs(ref[m]).max(), 1e-3)
+        assert np.abs(got[m] - ref[m]).max() <= tol * scale
+    assert np.abs(ko[m]).max() > 1e-4  # doubly curved
+    assert np.isnan(hh[z < 0]).all()
+
+
+def test_curvature_pass_sphere():
+    """Known answer: spherical level sets psi = cos(r - R) centred below the box:
+    H = 2/r and K = 1/r^2 at the crossing, to the accuracy of the reference's
+    difference gradients (dx = 2 pi / 32)."""
+    n = 64
+    dx = 2 * math.pi / 32
+    p = S.Params(n=n, dx=dx, boundary="neumann", precision="fp64", dt=0.01, eps=-0.7)
+    x = np.arange(n) * dx
+    L = n * dx
+    r = np.sqrt((x[:, None, None] - L / 2) ** 2 + (x[None, :, None] - L / 2) ** 2 + (x[None, None, :] + 12.0) ** 2)
+    psi0 = np.cos(r - 12.0 - 0.5 * L - 0.11)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        z, vn, hh, kk = s.surface_step()
+    for i, j in ((n // 2, n // 2), (n // 2 + 5, n // 2 - 7)):
+        assert z[i, j] >= 0
+        rr = r[i, j, z[i, j]]
+        assert abs(hh[i, j] * rr / 2 - 1) < 0.02
+        assert abs(kk[i, j] * rr * rr - 1) < 0.03

@@ -212,3 +212,45 @@ def test_golden_fixtures_reproduce():
                 assert np.allclose(got[k], ref[k], rtol=1e-12, atol=1e-14), (name, k)
             else:
                 assert (np.asarray(got[k]) == ref[k]).all(), (name, k)
+
+
+def test_curvature_pass_sphere_kat():
+    """Neumann curvature pass (cosNoAdvMorphCurv.cpp:874-965) on spherical level
+    sets psi = cos(r - R): Megrabov's H = 2/r and K = 1/r^2 at the crossing,
+    to the accuracy of the difference gradients (dx = 2 pi / 32)."""
+    n = 48
+    dx = 2 * math.pi / 32
+    p = O.Params(n=n, dx=dx, dt=0.05, eps=-0.7)
+    x = np.arange(n) * dx
+    L = n * dx
+    r = np.sqrt((x[:, None, None] - L / 2) ** 2 + (x[None, :, None] - L / 2) ** 2 + (x[None, None, :] + 12.0) ** 2)
+    psi = np.cos(r - 12.0 - 0.5 * L)
+    orc = O.NeumannOracle(psi, p)
+    z, vn, hh, kk = O.neumann_curvature_scan(psi, O.neumann_curvature_fields(orc), dx)
+    i = j = n // 2
+    rr = r[i, j, z[i, j]]
+    assert abs(hh[i, j] * rr / 2 - 1) < 0.02
+    assert abs(kk[i, j] * rr * rr - 1) < 0.03
+
+
+def test_curvature_pass_plane_is_flat():
+    """Planar lamellae psi = cos(z - phi): H = K = 0 and v_n = d_t psi / |psi_z|."""
+    n = 16
+    p = O.Params(n=n, dt=0.05, eps=-0.7)
+    z = np.arange(n) * p.dx
+    psi = np.broadcast_to(1.3 * np.cos(z - 0.37)[None, None, :], (n, n, n)).copy()
+    orc = O.NeumannOracle(psi, p)
+    zz, vn, hh, kk = O.neumann_curvature_scan(psi, O.neumann_curvature_fields(orc), p.dx)
+    assert (zz >= 0).all() and (zz == zz[0, 0]).all()
+    assert np.abs(hh).max() < 1e-12 and np.abs(kk).max() < 1e-12
+
+
+def test_substrate_zero_sigma_is_plain_neumann():
+    """sigma = 0 (the reference's setting) leaves the Neumann step unchanged."""
+    n = 16
+    psi0 = np.cos(np.arange(n) * 2 * math.pi / 8)[None, None, :] + 0.1 * np.random.default_rng(1).uniform(-1, 1, (n, n, n))
+    a = O.NeumannOracle(psi0, O.Params(n=n, dt=0.05, sub_sigma=0.0, sub_z0=2.0))
+    b = O.NeumannOracle(psi0, O.Params(n=n, dt=0.05))
+    a.run(5)
+    b.run(5)
+    assert np.array_equal(a.psi, b.psi)

@@ -37,8 +37,6 @@ def oracle_params(p: S.Params) -> O.Params:
 def golden(name):
     d = np.load(os.path.join(GOLDEN, name + ".npz"))
     kw = {k[6:]: d[k].item() for k in d.files if k.startswith("param_")}
-    kw.pop("sub_sigma", None)
-    kw.pop("sub_z0", None)
     return d, kw
 
 
@@ -51,6 +49,7 @@ def golden(name):
     ("neumann_hyperboloid_16", "neumann"),
     ("neumann_l1_32", "neumann"),
     ("periodic_advected_16", "periodic"),
+    ("neumann_substrate_16", "neumann"),
 ])
 def test_golden_vectors(name, boundary, prec):
     d, kw = golden(name)
