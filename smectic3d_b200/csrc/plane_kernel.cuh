@@ -116,21 +116,17 @@ struct PlaneArgs {
   int kwall;
 };
 
-// Cluster barrier.  RELEASE orders this thread's earlier shared-memory writes
-// (local and remote) before the peers' reads; without it the barrier only
-// orders execution, which is what a write-after-read hand-over needs.
-template <int CL, bool RELEASE>
-__device__ __forceinline__ void cluster_sync() {
-  if constexpr (CL == 1) {
-    __syncthreads();
-  } else {
-    if constexpr (RELEASE) {
-      asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
-    } else {
-      asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
-    }
-    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
-  }
+// Split cluster barrier.  A CTA arrives as soon as it no longer reads its
+// receive blocks (and, at the start, once its mbarriers are initialised); it
+// waits only right before copying into its peers' receive blocks.  The work
+// between the two hides the skew between the CTAs of a cluster.
+template <int CL>
+__device__ __forceinline__ void cluster_arrive() {
+  if constexpr (CL > 1) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+}
+template <int CL>
+__device__ __forceinline__ void cluster_wait() {
+  if constexpr (CL > 1) asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
 }
 
 // shared::cluster address of ``p`` in the copy of this CTA's shared memory
@@ -155,11 +151,14 @@ struct Xchg {
 
 // Every thread has written its share of the send blocks; copy block d to CTA d
 // (cp.async.bulk shared::cta -> shared::cluster, completing on the receiver's
-// mbarrier ``which``) and wait until all CL incoming blocks have landed.
+// mbarrier ``which``) and wait until all CL incoming blocks have landed.  The
+// caller has arrived at the cluster barrier since it last read its receive
+// blocks (cluster_arrive).
 template <typename T, int CL>
 __device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, int blk) {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  cluster_sync<CL, true>();  // send blocks complete here, receive blocks free everywhere
+  __syncthreads();     // every thread's send-block writes precede the copies
+  cluster_wait<CL>();  // every peer has arrived: its receive blocks are free, its mbarriers initialised
   if (threadIdx.x == 0) {
     const uint32_t bytes = uint32_t(blk * sizeof(cplx<T>));
     const uint32_t mb = smem_u32(&x.mbar[which]);
@@ -669,12 +668,12 @@ plane_kernel(PlaneArgs<T> a) {
     xs.phases = 0;
     xs.timeout = a.timeout;
     if (threadIdx.x == 0) {
-      // peers see the initialised barriers after the cluster barrier that opens
-      // the first exchange
+      // peers see the initialised barriers once they have waited on the arrive below
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[0])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[1])) : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    cluster_arrive<CL>();  // matched by the wait of the first exchange
   }
   const int x = blockIdx.x / CL;
   const int rep = blockIdx.y;
@@ -693,6 +692,8 @@ plane_kernel(PlaneArgs<T> a) {
     }
     Ops::col_inverse_to_rows(buf, xs, rank, tw);
     Ops::row_inverse(v, buf, xs, L, line, t, tw);
+    // done with the receive blocks; the step and the adjoint exchange once more
+    if constexpr (MODE == kPlaneStep || MODE == kPlaneAdj) cluster_arrive<CL>();
 
     if (a.flags & (kFlPsiOut | kFlL1 | kFlEnergy)) {
       KahanSum s0, s1, s2;
@@ -844,6 +845,7 @@ plane_kernel(PlaneArgs<T> a) {
         }
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, (field == 0 ? a.dst2 : a.dst) + plane_off, rank, tw);
+      if (field == 0) cluster_arrive<CL>();  // done with the receive blocks before the second exchange
     }
   }
   if constexpr (CL > 1) {
