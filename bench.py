@@ -297,6 +297,7 @@ def run_ours(args, rank, world, local_rank, dist):
            "api": "smectic3d_b200.Solver.run -> sh_run (pinned host psi in, K steps with the L1 monitor every 100, psi out)"}
 
     adj = adjoint_ratio(args, torch) if args.adjoint_steps > 0 else None
+    others = other_configs(torch) if (world == 1 and args.other_configs) else None
 
     if rank != 0:
         return None
@@ -326,6 +327,7 @@ def run_ours(args, rank, world, local_rank, dist):
                             "rel_err_fp32_vs_fp64_after_100_steps": acc100},
         "adjoint_forward_ratio": adj["backward_over_forward"] if adj else None,
         "adjoint": adj,
+        "other_configs": others,
     }
     return line
 
@@ -361,6 +363,72 @@ def adjoint_ratio(args, torch):
             "forward_ms_per_step": t_fwd / t_steps * 1e3, "adjoint_ms_per_step": t_adj / t_steps * 1e3,
             "total_over_forward": t_adj / t_fwd, "backward_over_forward": (t_adj - t_fwd) / t_fwd,
             "grad_eps": float(ge[0]), "grad_q0": float(gq[0])}
+
+
+def other_configs(torch, steps=200):
+    """Device-timed steps/s of the other synthetic configurations (seeded inputs):
+    C1 periodic 128^3 FP64; C3 periodic 256^3 FP32 with Stokes advection, dt=0.02,
+    undulated lamellae, the surfTrack pass every 10 steps (host-timed, since each
+    pass returns its surface to the host); C4 64 replicas x 64^3 FP32 with
+    eps_r = linspace(-0.9, -0.5, 64).  Each reports steps/s and the HBM roofline
+    fraction of its algorithmic bytes per step (SURVEY-style model: periodic
+    2R + 4H, advected 8R + 12H)."""
+    import numpy as np
+    import smectic3d_b200 as S
+    peak, _ = peaks()
+    out = {}
+
+    def model_bytes(n, batch, prec, advect):
+        s_ = 4 if prec == "fp32" else 8
+        r_, h_ = s_ * n ** 3, 2 * s_ * n * n * (n // 2 + 1)
+        return batch * ((8 * r_ + 12 * h_) if advect else (2 * r_ + 4 * h_))
+
+    # C1 and C4: plain steps, CUDA events on the solver stream
+    for name, p, psi in (
+            ("C1 periodic 128^3 fp64", S.Params(n=128, precision="fp64", dt=0.05, eps=-0.75), S.ic.noise(128, 0)),
+            ("C4 64 x 64^3 fp32", S.Params(n=64, batch=64, precision="fp32", dt=0.05, eps=-0.75,
+                                           eps_per_replica=tuple(np.linspace(-0.9, -0.5, 64))),
+             S.ic.noise_batch(64, range(64)))):
+        with S.Solver(p) as s:
+            s.set_psi(psi)
+            s.step(10)
+            ms = timed_steps(s, steps, torch, None)
+        rate = steps / (ms / 1e3)
+        b = model_bytes(p.n, p.batch, p.precision, False)
+        out[name] = {"steps_per_s": rate, "us_per_step": 1e3 * ms / steps,
+                     "roofline_frac": b * rate / (peak * 1e9)}
+    # C3: advected, surfTrack every 10 steps
+    n = 256
+    p = S.Params(n=n, precision="fp32", dt=0.02, eps=-0.75, advection=True)
+    with S.Solver(p) as s:
+        s.set_psi(S.ic.undulated_lamellae(n, p.dx, seed=0))
+        s.step(3)
+        s.synchronize()
+        nblk = max(1, steps // 20)
+        t0 = time.perf_counter()
+        found = 0
+        for _ in range(nblk):
+            z, _vn, _hh, _kk = s.surface_step()
+            found = int((z >= 0).sum())
+            s.step(9)
+        s.synchronize()
+        t1 = time.perf_counter()
+        rate = 10 * nblk / (t1 - t0)
+        s.step(3)
+        s.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ext = torch.cuda.ExternalStream(s.stream)
+        ev0.record(ext)
+        s.step_async(20)
+        ev1.record(ext)
+        ev1.synchronize()
+        plain = 20 / (ev0.elapsed_time(ev1) / 1e3)
+    b = model_bytes(n, 1, "fp32", True)
+    out["C3 advected 256^3 fp32 + surfTrack/10"] = {
+        "steps_per_s": rate, "us_per_step": 1e6 / rate, "steps_per_s_without_surface": plain,
+        "roofline_frac": b * plain / (peak * 1e9), "surface_columns_found": found,
+        "timing": "host clock around 10-step blocks (each surface pass returns to the host)"}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -428,6 +496,8 @@ def main():
     ap.add_argument("--workload", default="neumann256", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--adjoint-steps", type=int, default=1000, help="steps of the adjoint ratio (0 = skip)")
+    ap.add_argument("--no-other-configs", dest="other_configs", action="store_false",
+                    help="skip the C1 / C3 / C4 measurements reported beside the headline")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
