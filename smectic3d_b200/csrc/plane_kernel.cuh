@@ -26,14 +26,17 @@
 
 namespace shb {
 
-enum PlaneMode : int { kPlaneStep = 0, kPlaneInit = 1, kPlaneGetPsi = 2, kPlaneInvReal = 3, kPlaneFwdReal = 4, kPlaneAdj = 5 };
+enum PlaneMode : int {
+  kPlaneStep = 0,
+  kPlaneInit = 1,
+  kPlaneGetPsi = 2,
+  kPlaneInvReal = 3,
+  kPlaneAdj = 5,
+  kPlaneInvMulFwd = 6,  // inverse of (mult x src) -> real_out; times real_in[0]; forward -> dst
+  kPlaneAdvN = 7,       // N(real_in[0]) - sum_c (inverse of src3[c]) real_in[1+c]; forward -> dst
+};
 // spectral multiplier applied to the partial spectrum as the plane is loaded
 enum SpecMult : int { kMulNone = 0, kMulIqy = 1, kMulIqz = 2, kMulNegQy2 = 3, kMulNegQz2 = 4 };
-// real-space operation of kPlaneFwdReal
-enum RealOp : int {
-  kOpProduct = 0,   // in[0] * in[1]                      (stress S_i = (L psi) d_i psi)
-  kOpAdvected = 1,  // N(in[0]) + penalty - sum_i in[4+i] in[1+i]  (nonlinearity with -u.grad psi)
-};
 
 
 template <typename T, int N, int CL, bool DCT>
@@ -83,6 +86,8 @@ struct PlaneCfg {
 #endif
   static constexpr int MIN_BLOCKS =
       (SHB_PLANE_THREE && sizeof(T) == 4 && CL > 1 && THREADS == 256 && SMEM <= 76800) ? 3 : 0;
+  // kPlaneAdvN keeps an accumulator beside the transform registers: no cap
+  static constexpr int min_blocks(int mode) { return mode == kPlaneAdvN ? 0 : MIN_BLOCKS; }
   static_assert(THREADS % 32 == 0, "plane CTA must be whole warps");
 };
 
@@ -102,7 +107,6 @@ struct PlaneArgs {
   // real-field modes: wavenumber table, multiplier, real inputs / output
   const T* q;
   int mult;
-  int op;
   const T* real_in[7];
   T* real_out;
   // kPlaneInvReal: optional second partial, added after its own multiplier
@@ -114,6 +118,8 @@ struct PlaneArgs {
   const T* wall;
   const T* lperp;
   int kwall;
+  // kPlaneAdvN: the three velocity partials
+  const cplx<T>* src3[3];
 };
 
 // Split cluster barrier.  A CTA arrives as soon as it no longer reads its
@@ -645,7 +651,7 @@ __device__ __forceinline__ void row_nonlin(cplx<T> (&v)[Plan<N>::E], cplx<T>* L,
 }
 
 template <typename T, int N, int CL, bool DCT, int MODE>
-__global__ void __launch_bounds__(PlaneCfg<T, N, CL, DCT>::THREADS, PlaneCfg<T, N, CL, DCT>::MIN_BLOCKS)
+__global__ void __launch_bounds__(PlaneCfg<T, N, CL, DCT>::THREADS, PlaneCfg<T, N, CL, DCT>::min_blocks(MODE))
 plane_kernel(PlaneArgs<T> a) {
   using Cfg = PlaneCfg<T, N, CL, DCT>;
   using Ops = PlaneOps<T, N, CL, DCT>;
@@ -684,8 +690,9 @@ plane_kernel(PlaneArgs<T> a) {
   const int y0 = rank * ROWS + 2 * line;
   cplx<T> v[E];
 
-  if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi || MODE == kPlaneInvReal || MODE == kPlaneAdj) {
-    if constexpr (MODE == kPlaneInvReal) {
+  if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi || MODE == kPlaneInvReal || MODE == kPlaneAdj ||
+                MODE == kPlaneInvMulFwd) {
+    if constexpr (MODE == kPlaneInvReal || MODE == kPlaneInvMulFwd) {
       Ops::col_load(buf, a.src + plane_off, rank, a.mult, a.q, a.src2 ? a.src2 + plane_off : nullptr, a.mult2);
     } else {
       Ops::col_load(buf, a.src + plane_off, rank);
@@ -693,7 +700,7 @@ plane_kernel(PlaneArgs<T> a) {
     Ops::col_inverse_to_rows(buf, xs, rank, tw);
     Ops::row_inverse(v, buf, xs, L, line, t, tw);
     // done with the receive blocks; the step and the adjoint exchange once more
-    if constexpr (MODE == kPlaneStep || MODE == kPlaneAdj) cluster_arrive<CL>();
+    if constexpr (MODE == kPlaneStep || MODE == kPlaneAdj || MODE == kPlaneInvMulFwd) cluster_arrive<CL>();
 
     if (a.flags & (kFlPsiOut | kFlL1 | kFlEnergy)) {
       KahanSum s0, s1, s2;
@@ -744,7 +751,7 @@ plane_kernel(PlaneArgs<T> a) {
             o0[zn + z] = v[b * RL + r].y;
           }
         }
-    } else if (MODE == kPlaneInvReal || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
+    } else if (MODE == kPlaneInvReal || MODE == kPlaneInvMulFwd || (MODE == kPlaneStep && (a.flags & kFlRealOut))) {
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -771,44 +778,67 @@ plane_kernel(PlaneArgs<T> a) {
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
     }
+    if constexpr (MODE == kPlaneInvMulFwd) {
+      // stress component S_c = (L psi) d_c psi (periodicFFT/pf3d.cpp:417-429), formed
+      // from the derivative just written and sent forward in the same pass
+      const T* f = a.real_in[0];
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const size_t ia = real_off + size_t(y0) * N + Ops::row_z(t, b, r);
+          v[b * RL + r] = mk<T>(v[b * RL + r].x * f[ia], v[b * RL + r].y * f[ia + N]);
+        }
+      Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
+      Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
+    }
     if constexpr (MODE == kPlaneStep) {
       const T* lp0 = a.kwall > 0 ? a.lperp + ((size_t(rep) * N + x) * N + y0) * a.kwall : nullptr;
       row_nonlin<T, N, CL, DCT>(v, L, t, a.pp, a.wall, lp0, a.kwall);
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
     }
-  } else if constexpr (MODE == kPlaneFwdReal) {
-    // real fields -> pointwise op -> partial spectrum
-    constexpr int R0 = radix_of<N, -1, 0>();
+  } else if constexpr (MODE == kPlaneAdvN) {
+    // N = beta psi^3 - gamma psi^5 (+ pinning) - u . grad psi (periodicFFT/pf3d.cpp:455-467):
+    // the velocity components come in as partials and are inverted here one
+    // after the other, u_c d_c psi accumulating in registers
+    cplx<T> acc[E];
+#pragma unroll
+    for (int e = 0; e < E; ++e) acc[e] = mk<T>(T(0), T(0));
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      if (c > 0) __syncthreads();  // every line has left the line buffer
+      Ops::col_load(buf, a.src3[c] + plane_off, rank);
+      Ops::col_inverse_to_rows(buf, xs, rank, tw);
+      Ops::row_inverse(v, buf, xs, L, line, t, tw);
+      cluster_arrive<CL>();  // done with the receive blocks; another exchange follows
+      const T* d = a.real_in[1 + c];
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const size_t ia = real_off + size_t(y0) * N + Ops::row_z(t, b, r);
+          acc[b * RL + r].x = fma(v[b * RL + r].x, d[ia], acc[b * RL + r].x);
+          acc[b * RL + r].y = fma(v[b * RL + r].y, d[ia + N], acc[b * RL + r].y);
+        }
+    }
     const T beta = T(a.pp.beta), gamma = T(a.pp.gamma);
     const T cpen = T(2.0 * a.pp.w_mid * a.pp.inv_dz2);
+    const T* ps = a.real_in[0];
 #pragma unroll
-    for (int b = 0; b < E / R0; ++b)
+    for (int b = 0; b < E / RL; ++b)
 #pragma unroll
-      for (int r = 0; r < R0; ++r) {
-        const int n = in_index<N, -1>(t, b, r);
-        const int z = DCT ? mk_perm<N>(n) : n;
+      for (int r = 0; r < RL; ++r) {
+        const int z = Ops::row_z(t, b, r);
         const size_t ia = real_off + size_t(y0) * N + z, ib = ia + N;
-        T oa, ob;
-        if (a.op == kOpProduct) {
-          oa = a.real_in[0][ia] * a.real_in[1][ia];
-          ob = a.real_in[0][ib] * a.real_in[1][ib];
-        } else {
-          const T* ps = a.real_in[0];
-          const T pa = ps[ia], pb = ps[ib];
-          oa = nonlin_eval<T>(pa, beta, gamma, a.pp.nonlin);
-          ob = nonlin_eval<T>(pb, beta, gamma, a.pp.nonlin);
-          if (a.pp.w_mid != 0.0 && z == N / 2) {
-            oa += cpen * (ps[ia - 1] - T(2) * pa + ps[ia + 1]);
-            ob += cpen * (ps[ib - 1] - T(2) * pb + ps[ib + 1]);
-          }
-#pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            oa -= a.real_in[4 + c][ia] * a.real_in[1 + c][ia];
-            ob -= a.real_in[4 + c][ib] * a.real_in[1 + c][ib];
-          }
+        const T pa = ps[ia], pb = ps[ib];
+        T oa = nonlin_eval<T>(pa, beta, gamma, a.pp.nonlin);
+        T ob = nonlin_eval<T>(pb, beta, gamma, a.pp.nonlin);
+        if (a.pp.w_mid != 0.0 && z == N / 2) {
+          oa += cpen * (ps[ia - 1] - T(2) * pa + ps[ia + 1]);
+          ob += cpen * (ps[ib - 1] - T(2) * pb + ps[ib + 1]);
         }
-        v[b * R0 + r] = mk<T>(oa, ob);
+        v[b * RL + r] = mk<T>(oa - acc[b * RL + r].x, ob - acc[b * RL + r].y);
       }
     Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
     Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);

@@ -120,6 +120,7 @@ struct Solver final : SolverBase {
   T* CR[5] = {};
   cplx<T>* Psc = nullptr;
   bool real_fields_current = false;
+  bool u_real_current = false;
   // adjoint work buffers, kept for the handle's lifetime once allocated
   struct AdjBufs {
     cplx<T>* ck = nullptr;   // checkpoints: nseg states x {W, P, Nt}
@@ -252,7 +253,6 @@ struct Solver final : SolverBase {
     if ((rc = set_attrs(plane_fn<kPlaneInit>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneGetPsi>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneInvReal>(), PC::SMEM, true))) return rc;
-    if ((rc = set_attrs(plane_fn<kPlaneFwdReal>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(pencil_fn<kPencilStep>(), QC::smem(kPencilStep), false))) return rc;
     if ((rc = set_attrs(pencil_fn<kPencilInit>(), QC::smem(kPencilInit), false))) return rc;
     if ((rc = set_attrs(pencil_fn<kPencilEnergy>(), QC::smem(kPencilEnergy), false))) return rc;
@@ -265,6 +265,8 @@ struct Solver final : SolverBase {
     if ((rc = set_attrs(pencil_fn<kPencilAdj>(), QC::smem(kPencilAdj), false))) return rc;
     if ((rc = set_attrs(pencil_fn<kPencilAdjOut>(), QC::smem(kPencilAdjOut), false))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneAdj>(), PC::SMEM, true))) return rc;
+    if ((rc = set_attrs(plane_fn<kPlaneInvMulFwd>(), PC::SMEM, true))) return rc;
+    if ((rc = set_attrs(plane_fn<kPlaneAdvN>(), PC::SMEM, true))) return rc;
     return SH_OK;
   }
 
@@ -505,13 +507,13 @@ struct Solver final : SolverBase {
       return SH_EINVAL;
     } else {
       int rc;
-      const cplx<T>* src[5] = {P, Px, P, P, PSH};
-      const int mult[5] = {kMulNone, kMulNone, kMulIqy, kMulIqz, kMulNone};
-      for (int i = 0; i < 5; ++i) {
+      // psi and L psi to real space
+      const cplx<T>* src[2] = {P, PSH};
+      const int out[2] = {0, 4};
+      for (int i = 0; i < 2; ++i) {
         PlaneArgs<T> a = plane_args();
         a.src = src[i];
-        a.mult = mult[i];
-        a.real_out = R[i];
+        a.real_out = R[out[i]];
         if (i == 0) {
           a.flags = diag;
           a.psi_old = d_stash;
@@ -519,13 +521,17 @@ struct Solver final : SolverBase {
         }
         if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
       }
+      // grad psi to real space, and in the same pass the stress S_c = (L psi) d_c psi forward
+      const cplx<T>* dsrc[3] = {Px, P, P};
+      const int dmult[3] = {kMulNone, kMulIqy, kMulIqz};
       for (int c = 0; c < 3; ++c) {
         PlaneArgs<T> a = plane_args();
-        a.op = kOpProduct;
+        a.src = dsrc[c];
+        a.mult = dmult[c];
+        a.real_out = R[1 + c];
         a.real_in[0] = R[4];
-        a.real_in[1] = R[1 + c];
         a.dst = S3[c];
-        if ((rc = launch_plane<kPlaneFwdReal>(a))) return rc;
+        if ((rc = launch_plane<kPlaneInvMulFwd>(a))) return rc;
       }
       PencilArgs<T> b = pencil_args();
       for (int c = 0; c < 3; ++c) {
@@ -533,21 +539,28 @@ struct Solver final : SolverBase {
         b.u3[c] = S3[c];
       }
       if ((rc = launch_pencil<kPencilStokes>(b))) return rc;
-      for (int c = 0; c < 3; ++c) {
-        PlaneArgs<T> a = plane_args();
-        a.src = S3[c];
-        a.real_out = R[5 + c];
-        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
-      }
+      // N = beta psi^3 - gamma psi^5 - u . grad psi, the velocity inverted inside the pass
       PlaneArgs<T> a = plane_args();
-      a.op = kOpAdvected;
       for (int i = 0; i < 4; ++i) a.real_in[i] = R[i];
-      for (int c = 0; c < 3; ++c) a.real_in[4 + c] = R[5 + c];
+      for (int c = 0; c < 3; ++c) a.src3[c] = S3[c];
       a.dst = Nt;
-      if ((rc = launch_plane<kPlaneFwdReal>(a))) return rc;
+      if ((rc = launch_plane<kPlaneAdvN>(a))) return rc;
       real_fields_current = true;
+      u_real_current = false;  // the velocity stays spectral (S3) unless a surface pass needs it
       return SH_OK;
     }
+  }
+  // velocity of the current state in real space (R[5..7]) from its partials in S3
+  int velocity_real() {
+    int rc;
+    for (int c = 0; c < 3; ++c) {
+      PlaneArgs<T> a = plane_args();
+      a.src = S3[c];
+      a.real_out = R[5 + c];
+      if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+    }
+    u_real_current = true;
+    return SH_OK;
   }
 
   int psi_to_dpsi() override {
@@ -855,6 +868,7 @@ struct Solver final : SolverBase {
         for (auto& d : d_surf) SHB_CUDA(cudaMalloc(&d, nc * sizeof(double)));
       }
       if (!real_fields_current && (rc = adv_nonlinear(0))) return rc;
+      if (!u_real_current && (rc = velocity_real())) return rc;
       // second derivatives of psi^n: psi_xx = C2R(-q_x^2 psihat), psi_yy, psi_xy
       PencilArgs<T> b = pencil_args();
       b.src = Px;
