@@ -120,6 +120,14 @@ int sh_l1(sh_handle* h, double* out, int* count);
  *   Megrabov's H and K), then takes one step. */
 int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kgauss);
 
+/* Local-amplitude map of the current psi (cosFFT/comet/morphSurfAmp.cpp:
+ * 1005-1125): psiAvg = trapezoid integral of psi^2 over the box of +-Nw/2
+ * cells around each point (clipped at the grid edge), divided by the same
+ * integral over the box [Nw/2, 3 Nw/2]^3 times the box volume / (2 pi/q0)^3.
+ * Writes N^3 doubles per replica, dense (i, j, k) order.  Needs
+ * 3 (Nw/2) <= N - 1. */
+int sh_local_amplitude(sh_handle* h, int nw, double* out);
+
 /* Discrete adjoint of the CNAB2 loop (plain periodic step, SH_CNAB2, no
  * advection or penalty).  Integrates `nsteps` steps from psi0, then runs the
  * reverse sweep for a loss L whose gradient with respect to psi^T is

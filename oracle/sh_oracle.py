@@ -459,6 +459,68 @@ def neumann_curvature_scan(psi, f, dx: float, threshold: float = 0.7):
     return z, vn, hh, kk
 
 
+def _trapz(nstart, nend, h, vals):
+    """trapz of morphSurfAmp.cpp:76-86: 0.5 h sum_{n < nend - nstart} (v[n] + v[n+1])."""
+    t = 0.0
+    for m in range(nend - nstart):
+        t += vals[m] + vals[m + 1]
+    return 0.5 * h * t
+
+
+def local_amplitude_direct(psi, dx: float, nw: int, q0: float = 1.0):
+    """psiAvg of morphSurfAmp.cpp:1005-1125, loop for loop (small grids only)."""
+    n = psi.shape[0]
+    nl = nw // 2
+
+    def box(i0, i1, j0, j1, k0, k1):
+        az = []
+        for k2 in range(k0, k1 + 1):
+            ay = []
+            for j2 in range(j0, j1 + 1):
+                ax = [psi[i2, j2, k2] ** 2 for i2 in range(i0, i1 + 1)]
+                ay.append(_trapz(i0, i1, dx, ax))
+            az.append(_trapz(j0, j1, dx, ay))
+        return _trapz(k0, k1, dx, az)
+
+    ref = box(nl, 3 * nl, nl, 3 * nl, nl, 3 * nl)
+    lam3 = (2 * np.pi / q0) ** 3
+    out = np.empty_like(psi)
+    for i in range(n):
+        i0, i1 = max(i - nl, 0), min(i + nl, n - 1)
+        for j in range(n):
+            j0, j1 = max(j - nl, 0), min(j + nl, n - 1)
+            for k in range(n):
+                k0, k1 = max(k - nl, 0), min(k + nl, n - 1)
+                vol = (i1 - i0) * dx * (j1 - j0) * dx * (k1 - k0) * dx
+                out[i, j, k] = box(i0, i1, j0, j1, k0, k1) / (ref * vol / lam3)
+    return out
+
+
+def _window_trapz(f, axis, nl, h):
+    """Clipped-window trapezoid along ``axis``: h (sum f[a..b] - (f[a] + f[b]) / 2),
+    a = max(0, p - nl), b = min(n - 1, p + nl)."""
+    f = np.moveaxis(f, axis, 0)
+    n = f.shape[0]
+    c = np.concatenate([np.zeros((1,) + f.shape[1:]), np.cumsum(f, axis=0)])
+    p = np.arange(n)
+    a, b = np.maximum(p - nl, 0), np.minimum(p + nl, n - 1)
+    return np.moveaxis(h * (c[b + 1] - c[a] - 0.5 * (f[a] + f[b])), 0, axis)
+
+
+def local_amplitude(psi, dx: float, nw: int, q0: float = 1.0):
+    """psiAvg of morphSurfAmp.cpp:1005-1125 through the separable form of its
+    nested trapezoids (the box is a product domain); equals
+    local_amplitude_direct up to rounding."""
+    n = psi.shape[0]
+    nl = nw // 2
+    t = _window_trapz(_window_trapz(_window_trapz(psi * psi, 0, nl, dx), 1, nl, dx), 2, nl, dx)
+    ref = t[2 * nl, 2 * nl, 2 * nl]
+    p = np.arange(n)
+    ln = (np.minimum(p + nl, n - 1) - np.maximum(p - nl, 0)) * dx
+    vol = ln[:, None, None] * ln[None, :, None] * ln[None, None, :]
+    return t / (ref * vol / (2 * np.pi / q0) ** 3)
+
+
 # ---------------------------------------------------------------------------
 # diagnostics
 # ---------------------------------------------------------------------------

@@ -22,7 +22,7 @@ SH_LAYOUT_DENSE, SH_LAYOUT_PADDED = 0, 1
 EXPORTS = (
     "sh_default_params", "sh_create", "sh_destroy", "sh_set_psi", "sh_set_psi_device", "sh_get_psi",
     "sh_get_psi_device", "sh_step", "sh_step_async", "sh_run", "sh_energy", "sh_energy_trace", "sh_l1",
-    "sh_surface_step", "sh_adjoint", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
+    "sh_surface_step", "sh_local_amplitude", "sh_adjoint", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
     "sh_l1_noalloc", "sh_profile_steps", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
 )
 
@@ -72,6 +72,7 @@ def load() -> C.CDLL:
         "sh_energy_trace": (C.c_int, [vp, dp, C.c_int, ip]),
         "sh_l1": (C.c_int, [vp, dp, ip]),
         "sh_surface_step": (C.c_int, [vp, ip, dp, dp, dp]),
+        "sh_local_amplitude": (C.c_int, [vp, C.c_int, dp]),
         "sh_adjoint": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, dp, dp, vp]),
         "sh_checkpoint_save": (C.c_int, [vp, vp, C.POINTER(C.c_size_t)]),
         "sh_checkpoint_load": (C.c_int, [vp, vp, C.c_size_t]),

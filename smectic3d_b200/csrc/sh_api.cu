@@ -4,6 +4,7 @@
 #include <memory>
 #include <string>
 
+#include "amplitude_kernel.cuh"
 #include "sh_solver.cuh"
 
 using namespace shb;
@@ -280,6 +281,33 @@ int sh_get_psi(sh_handle* h, double* host_psi, int layout) {
     API_CUDA(h, cudaStreamSynchronize(s->stream));
     from_dense(tmp.data(), host_psi, s->p.n, s->p.batch, layout);
   }
+  return SH_OK;
+}
+
+int sh_local_amplitude(sh_handle* h, int nw, double* out) {
+  if (!h || !h->s || !out) return fail(h, SH_EINVAL, "null argument");
+  SolverBase* s = h->s;
+  if (!s->ready) return fail(h, SH_ESTATE, "psi was never set");
+  const int n = s->p.n, nl = nw / 2;
+  if (nw < 2 || 3 * nl > n - 1) return fail(h, SH_EINVAL, "nw must satisfy 2 <= nw and 3 (nw / 2) <= n - 1");
+  int rc = s->psi_to_dpsi();
+  if (rc) return rc;
+  const size_t bytes = s->n3() * s->p.batch * sizeof(double);
+  for (auto& b : s->d_amp)
+    if (!b) API_CUDA(h, cudaMalloc(&b, bytes));
+  const dim3 lines((unsigned)((size_t(n) * n + 255) / 256), s->p.batch);
+  const double dx = s->p.dx;
+  // psi^2 -> x window -> y window -> z window (morphSurfAmp.cpp:1076-1107)
+  amp_window_kernel<<<lines, 256, 0, s->stream>>>(s->d_psi, s->d_amp[0], n, 0, nl, dx, 1);
+  amp_window_kernel<<<lines, 256, 0, s->stream>>>(s->d_amp[0], s->d_amp[1], n, 1, nl, dx, 0);
+  amp_window_kernel<<<lines, 256, 0, s->stream>>>(s->d_amp[1], s->d_amp[0], n, 2, nl, dx, 0);
+  const double lam = 2.0 * M_PI / s->p.q0;
+  amp_normalise_kernel<<<dim3(592, s->p.batch), 256, 0, s->stream>>>(s->d_amp[0], s->d_amp[1], n, nl, dx,
+                                                                      lam * lam * lam);
+  API_CUDA(h, cudaGetLastError());
+  s->launches += 4;
+  API_CUDA(h, cudaMemcpyAsync(out, s->d_amp[1], bytes, cudaMemcpyDeviceToHost, s->stream));
+  API_CUDA(h, cudaStreamSynchronize(s->stream));
   return SH_OK;
 }
 

@@ -45,6 +45,7 @@ struct SolverBase {
   double* d_red_spec = nullptr;
   double* d_scalar = nullptr;  // batch doubles
   double* d_trace = nullptr;   // energy trace of the current chunk
+  double* d_amp[2] = {nullptr, nullptr};  // local-amplitude map work fields (allocated on first use)
   int trace_cap = 0;
   std::vector<double> energy_trace;  // host copy, steps * batch
   std::vector<double> l1_last;
@@ -62,6 +63,8 @@ struct SolverBase {
     cudaFree(d_red_spec);
     cudaFree(d_scalar);
     cudaFree(d_trace);
+    cudaFree(d_amp[0]);
+    cudaFree(d_amp[1]);
     for (auto& e : prof_ev)
       if (e) cudaEventDestroy(e);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);

@@ -199,6 +199,13 @@ class Solver:
                                            kk.ctypes.data_as(C.POINTER(C.c_double))))
         return z, vn, hh, kk
 
+    def local_amplitude(self, nw: int) -> np.ndarray:
+        """Local-amplitude map psiAvg of the current psi (morphSurfAmp.cpp:1005-1125),
+        the same shape as get_psi()."""
+        out = np.empty(self.shape, dtype=np.float64)
+        self._chk(self.lib.sh_local_amplitude(self.h, int(nw), out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
     def adjoint(self, psi0: np.ndarray, nsteps: int, dl_dpsi_t: np.ndarray, ckpt_every: int = 50):
         """Discrete adjoint of the CNAB2 loop: returns (dL/d eps, dL/d q0, dL/d psi0)
         per replica for a loss with gradient dl_dpsi_t at psi^T."""

@@ -102,3 +102,22 @@ def test_curvature_pass_sphere():
         rr = r[i, j, z[i, j]]
         assert abs(hh[i, j] * rr / 2 - 1) < 0.02
         assert abs(kk[i, j] * rr * rr - 1) < 0.03
+
+
+@pytest.mark.parametrize("boundary,prec", [("neumann", "fp64"), ("neumann", "fp32"), ("periodic", "fp64")])
+def test_local_amplitude_matches_oracle(boundary, prec):
+    """sh_local_amplitude (morphSurfAmp.cpp:1005-1125) on the handle's own psi
+    against the oracle's separable trapezoids; the map is FP64 either way."""
+    n = 64
+    p = S.Params(n=n, boundary=boundary, precision=prec, dt=0.05, eps=-0.7)
+    with S.Solver(p) as s:
+        s.set_psi(undulated(n, p.dx) + S.ic.noise(n, 4, 0.1))
+        s.step(5)
+        psi = s.get_psi()
+        # Nw = grid cells per wavelength (dx = 2 pi / 8): the box spans one wavelength
+        amp = s.local_amplitude(8)
+        with pytest.raises(S.ShError):
+            s.local_amplitude(44)  # 3 (nw/2) > n - 1
+    ref = O.local_amplitude(psi, p.dx, 8)
+    assert np.abs(amp - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert 0.5 < np.median(amp) < 1.5

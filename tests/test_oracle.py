@@ -254,3 +254,25 @@ def test_substrate_zero_sigma_is_plain_neumann():
     a.run(5)
     b.run(5)
     assert np.array_equal(a.psi, b.psi)
+
+
+def test_local_amplitude_separable_equals_loops():
+    """morphSurfAmp.cpp:1005-1125: the separable window form of the nested
+    trapezoids equals the reference's loops."""
+    rng = np.random.default_rng(3)
+    n = 12
+    dx = 2 * math.pi / 8
+    psi = np.cos(np.arange(n) * dx)[None, None, :] + 0.3 * rng.uniform(-1, 1, (n, n, n))
+    a = O.local_amplitude(psi, dx, 6)
+    b = O.local_amplitude_direct(psi, dx, 6)
+    assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+
+
+def test_local_amplitude_of_uniform_lamellae_is_one():
+    """A box of one wavelength over uniform lamellae holds exactly the reference box's
+    weight: psiAvg = 1 everywhere."""
+    n = 32
+    dx = 2 * math.pi / 8
+    psi = np.broadcast_to(1.3 * np.cos(np.arange(n) * dx + 0.4)[None, None, :], (n, n, n))
+    m = O.local_amplitude(psi, dx, 8)
+    assert np.abs(m[4:-4, 4:-4, 4:-4] - 1).max() < 1e-12
