@@ -120,6 +120,7 @@ struct PlaneArgs {
   int kwall;
   // kPlaneAdvN: the three velocity partials
   const cplx<T>* src3[3];
+  int drop_exchange;  // test hook (see Xchg::drop)
 };
 
 // Split cluster barrier.  A CTA arrives as soon as it no longer reads its
@@ -153,6 +154,7 @@ struct Xchg {
   uint64_t* mbar;
   uint32_t phases;
   int* timeout;
+  int drop;  // test hook: rank 0 sends nothing in exchange 0, so its peers' bounded waits run out
 };
 
 // Every thread has written its share of the send blocks; copy block d to CTA d
@@ -169,7 +171,8 @@ __device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, i
     const uint32_t bytes = uint32_t(blk * sizeof(cplx<T>));
     const uint32_t mb = smem_u32(&x.mbar[which]);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes * CL) : "memory");
-    for (int d = 0; d < CL; ++d) {
+    const bool send = !(x.drop && rank == 0 && which == 0);
+    for (int d = 0; send && d < CL; ++d) {
       const uint32_t dst = dsmem_map(x.rb + size_t(rank) * blk, d);
       const uint32_t src = smem_u32(x.sb + size_t(d) * blk);
       const uint32_t rmb = dsmem_map(&x.mbar[which], d);
@@ -673,6 +676,7 @@ plane_kernel(PlaneArgs<T> a) {
     xs.mbar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::MB_OFF);
     xs.phases = 0;
     xs.timeout = a.timeout;
+    xs.drop = a.drop_exchange;
     if (threadIdx.x == 0) {
       // peers see the initialised barriers once they have waited on the arrive below
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[0])) : "memory");

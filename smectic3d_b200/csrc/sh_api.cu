@@ -205,6 +205,10 @@ int sh_create(const sh_params* p, sh_handle** out) {
     return SH_ENOMEM;
   }
   cudaMemset(s->d_flag, 0, 2 * sizeof(int));
+  {
+    const char* drop = getenv("SMECTIC_B200_TEST_DROP_EXCHANGE");
+    s->drop_exchange = (drop && drop[0] == '1') ? 1 : 0;
+  }
   cudaMemcpy(s->d_eps, s->eps.data(), p->batch * sizeof(double), cudaMemcpyHostToDevice);
   s->l1_last.assign(p->batch, 0.0);
   int rc = s->setup();

@@ -52,6 +52,11 @@ struct SolverBase {
   int l1_count = 0;
   bool ready = false;
   bool psi0_valid = false;  // d_psi holds psi^0 exactly as uploaded
+  // Test hook for the timeout path, from SMECTIC_B200_TEST_DROP_EXCHANGE=1 at
+  // sh_create: the first exchange of every plane pass of a cluster loses rank
+  // 0's copies, the bounded waits expire (about 1 s) and the call returns
+  // SH_ETIMEOUT.  Never set otherwise.
+  int drop_exchange = 0;
 
   virtual ~SolverBase() {
     if (stream) cudaStreamSynchronize(stream);
@@ -306,6 +311,7 @@ struct Solver final : SolverBase {
     a.pp = point_params();
     a.red = d_red_plane;
     a.timeout = d_flag + 1;
+    a.drop_exchange = drop_exchange;
     a.q = q;
     return a;
   }
