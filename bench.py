@@ -60,6 +60,11 @@ def params_for(workload, precision=None):
     return S.Params(n=n, batch=batch, boundary=bnd, precision=precision or prec, dt=0.05, eps=-0.75, **kw)
 
 
+def workload_label(workload):
+    bnd, n, batch, _, ick = WORKLOADS[workload]
+    return f"{workload}: {bnd} {n}^3 x{batch}, {ick} IC, dt=0.05, eps=-0.75, beta=2, gamma=1, q0=1, dx=2pi/8"
+
+
 def algorithmic_bytes(boundary, n, batch, precision):
     """Bytes one launch of each pass must move (read its inputs once, write
     its outputs once): pencil reads N-partial + W, writes W + psi-partial;
@@ -307,8 +312,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": k, "warmup": w,
         "ms_per_step": ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if prec == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": f"{args.workload}: {bnd} {n}^3 x{batch}, {WORKLOADS[args.workload][4]} IC, dt=0.05, "
-                               f"eps=-0.75, beta=2, gamma=1, q0=1, dx=2pi/8",
+        "config": {"workload": workload_label(args.workload),
                    "precision": prec, "parallelism": f"replicas x{world}",
                    "l2": f"inputs larger than L2: working set {3 * field_mb:.0f} MB > 126 MB, no flush"},
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -466,7 +470,7 @@ def run_reference(args, rank):
     if rank != 0:
         return None
     k = min(args.steps, 30)
-    w = min(args.warmup, 1)
+    w = min(args.warmup, 3)
     orc, batch = _oracle_solver(args.workload)
     for _ in range(w):
         orc.step()
@@ -482,7 +486,8 @@ def run_reference(args, rank):
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": k,
             "warmup": w, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.workload}: {bnd} {n}^3 x{batch}", "precision": "fp64 (CPU)"},
+            "config": {"workload": workload_label(args.workload), "precision": "fp64 (CPU oracle port)",
+                       "parallelism": f"{os.cpu_count()} host threads"},
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
 
