@@ -24,7 +24,8 @@
 namespace {
 
 struct Opts {
-  int n = 64, nw = 16, l1_every = 100, save_every = 100;
+  int n = 64, nw = 16, l1_every = 100, save_every = 100, surface_every = 0, amp_nw = 0;
+  double sub_sigma = 0.0, sub_z0 = 1e-4;
   long long max_steps = -1;
   double dt = 0.001, eps = -0.7, beta = 2.0, gamma = 1.0, alpha = 1.0, q0 = 1.0, eta = 1.0, rho = 1.0, w_mid = 0.0;
   double l1_limit = 1e-6;
@@ -37,7 +38,12 @@ void usage() {
       "usage: smectic_run [--n N] [--nw Nw] [--dt dt] [--eps e] [--beta b] [--gamma g] [--alpha a] [--q0 q]\n"
       "                   [--eta h] [--rho r] [--w-mid w] [--boundary periodic|neumann] [--advection]\n"
       "                   [--precision fp64|fp32] [--ic lamellae|torus|hyperboloid|load:FILE]\n"
-      "                   [--l1-limit x] [--l1-every k] [--save-every m] [--max-steps s] [--out DIR]");
+      "                   [--l1-limit x] [--l1-every k] [--save-every m] [--max-steps s] [--out DIR]\n"
+      "                   [--sub-sigma s] [--sub-z0 z0] [--surface-every m] [--amp-nw Nw]\n"
+      "  --surface-every m  every m-th L1 evaluation, end the block with the surface pass and append\n"
+      "                     surfPsi.dat, velSurf.dat, curvH.dat, curvK.dat (Neumann: all columns, keeping\n"
+      "                     the last value where no crossing is found; periodic: surfTrack, crossings only)\n"
+      "  --amp-nw Nw        at the end, write the local-amplitude map psiAvg.dat (morphSurfAmp)");
 }
 
 bool parse(int argc, char** argv, Opts& o) {
@@ -73,6 +79,10 @@ bool parse(int argc, char** argv, Opts& o) {
     else if (a == "--save-every") o.save_every = std::atoi(need("--save-every"));
     else if (a == "--max-steps") o.max_steps = std::atoll(need("--max-steps"));
     else if (a == "--out") o.out = need("--out");
+    else if (a == "--sub-sigma") o.sub_sigma = std::atof(need("--sub-sigma"));
+    else if (a == "--sub-z0") o.sub_z0 = std::atof(need("--sub-z0"));
+    else if (a == "--surface-every") o.surface_every = std::atoi(need("--surface-every"));
+    else if (a == "--amp-nw") o.amp_nw = std::atoi(need("--amp-nw"));
     else {
       std::fprintf(stderr, "unknown option %s\n", a.c_str());
       usage();
@@ -163,6 +173,8 @@ int main(int argc, char** argv) {
   p.advection = o.advection ? 1 : 0;
   p.precision = o.precision == "fp32" ? SH_FP32 : SH_FP64;
   p.l1_interval = o.l1_every;
+  p.sub_sigma = o.sub_sigma;
+  p.sub_z0 = o.sub_z0;
   sh_handle* h = nullptr;
   if (sh_create(&p, &h) != SH_OK) {
     std::fprintf(stderr, "sh_create: %s\n", sh_last_error(nullptr));
@@ -176,14 +188,49 @@ int main(int argc, char** argv) {
     return 1;
   }
   std::ofstream(o.out + "/L1.dat").close();
+  const size_t nc = size_t(o.n) * o.n;
+  std::vector<int> zc(nc);
+  std::vector<double> vn(nc), hh(nc), kk(nc), zs(nc, 0.0), vs(nc, 0.0), hs(nc, 0.0), ks(nc, 0.0);
+  if (o.surface_every > 0)
+    for (const char* f : {"/surfPsi.dat", "/velSurf.dat", "/curvH.dat", "/curvK.dat"}) std::ofstream(o.out + f).close();
   double l1 = 1.0;
   long long steps = 0;
-  int count_save = 0;
+  int count_save = 0, count_surf = 0;
   while (l1 > o.l1_limit && (o.max_steps < 0 || steps < o.max_steps)) {
     const int k = o.max_steps < 0 ? o.l1_every : int(std::min<long long>(o.l1_every, o.max_steps - steps));
-    if (sh_step(h, k) != SH_OK) {
+    const bool surf = o.surface_every > 0 && k == o.l1_every && ++count_surf == o.surface_every;
+    if (sh_step(h, surf ? k - 1 : k) != SH_OK) {
       std::fprintf(stderr, "sh_step: %s\n", sh_last_error(h));
       return 1;
+    }
+    if (surf) {  // the last step of the block goes through the surface pass
+      count_surf = 0;
+      if (sh_surface_step(h, zc.data(), vn.data(), hh.data(), kk.data()) != SH_OK) {
+        std::fprintf(stderr, "sh_surface_step: %s\n", sh_last_error(h));
+        return 1;
+      }
+      std::ofstream fz(o.out + "/surfPsi.dat", std::ios_base::app), fv(o.out + "/velSurf.dat", std::ios_base::app),
+          fh(o.out + "/curvH.dat", std::ios_base::app), fk(o.out + "/curvK.dat", std::ios_base::app);
+      for (size_t c = 0; c < nc; ++c) {
+        if (p.boundary == SH_NEUMANN) {
+          // cosNoAdvMorphCurv.cpp:995-1013: every column; a column without a crossing keeps its value
+          if (zc[c] >= 0) {
+            zs[c] = zc[c];
+            vs[c] = vn[c];
+            hs[c] = hh[c];
+            ks[c] = kk[c];
+          }
+          fz << zs[c] << "\n";
+          fv << vs[c] << "\n ";
+          fh << hs[c] << "\n ";
+          fk << ks[c] << "\n ";
+        } else if (zc[c] >= 0) {  // surfTrack.cpp:787-799: the columns with a crossing
+          fz << zc[c] << "\n ";
+          fv << vn[c] << "\n ";
+          fh << hh[c] << "\n ";
+          fk << kk[c] << "\n ";
+        }
+      }
     }
     steps += k;
     if (k < o.l1_every) break;  // partial last block: no L1 evaluation
@@ -198,6 +245,14 @@ int main(int argc, char** argv) {
   }
   sh_get_psi(h, psi.data(), SH_LAYOUT_DENSE);
   write_psi(o.out + "/psi.dat", psi);
+  if (o.amp_nw > 0) {
+    std::vector<double> amp(psi.size());
+    if (sh_local_amplitude(h, o.amp_nw, amp.data()) != SH_OK) {
+      std::fprintf(stderr, "sh_local_amplitude: %s\n", sh_last_error(h));
+      return 1;
+    }
+    write_psi(o.out + "/psiAvg.dat", amp);  // morphSurfAmp.cpp:1113-1122
+  }
   std::printf("steps %lld  L1 %.6g\n", steps, l1);
   sh_destroy(h);
   return 0;

@@ -47,6 +47,8 @@ def test_surface_files(tmp_path):
 def test_driver_help_and_bad_option():
     r = subprocess.run([DRIVER, "--help"], capture_output=True, text=True)
     assert r.returncode == 0 and "usage" in r.stdout
+    for flag in ("--sub-sigma", "--surface-every", "--amp-nw"):
+        assert flag in r.stdout
     r = subprocess.run([DRIVER, "--bogus"], capture_output=True, text=True)
     assert r.returncode == 2
 
@@ -71,3 +73,24 @@ def test_driver_matches_python_api(tmp_path):
     got = sio.read_psi_text(tmp_path / "psi.dat", n)
     assert np.allclose(got, ref, rtol=1e-5, atol=1e-5)
     assert abs(l1[-1] - l1_ref[0]) <= 1e-5 * abs(l1_ref[0])
+
+
+@pytest.mark.gpu
+def test_driver_neumann_surface_and_amplitude(tmp_path):
+    """cosNoAdvMorphCurv-style run: the surface files hold every column at each
+    save, psiAvg.dat is the local-amplitude map of the final psi."""
+    import smectic3d_b200 as S
+    n = 32
+    r = subprocess.run([DRIVER, "--n", str(n), "--nw", "8", "--dt", "0.05", "--eps", "-0.7", "--ic", "hyperboloid",
+                        "--boundary", "neumann", "--sub-sigma", "0.3", "--sub-z0", "1.5", "--l1-every", "5",
+                        "--surface-every", "2", "--max-steps", "20", "--amp-nw", "8", "--out", str(tmp_path)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    z = np.loadtxt(tmp_path / "surfPsi.dat")
+    assert z.size == 2 * n * n  # two saves (blocks 2 and 4), every column
+    assert np.isfinite(np.loadtxt(tmp_path / "curvH.dat")).all()
+    psi = sio.read_psi_text(tmp_path / "psi.dat", n)
+    amp = sio.read_psi_text(tmp_path / "psiAvg.dat", n)
+    from oracle import sh_oracle as O
+    ref = O.local_amplitude(psi, 2 * np.pi / 8, 8)
+    assert np.allclose(amp, ref, rtol=1e-4, atol=1e-5)  # psi.dat and psiAvg.dat carry 6 digits
