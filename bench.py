@@ -375,8 +375,8 @@ def other_configs(torch, steps=200):
     undulated lamellae, the surfTrack pass every 10 steps (host-timed, since each
     pass returns its surface to the host); C4 64 replicas x 64^3 FP32 with
     eps_r = linspace(-0.9, -0.5, 64).  Each reports steps/s and the HBM roofline
-    fraction of its algorithmic bytes per step (SURVEY-style model: periodic
-    2R + 4H, advected 8R + 12H)."""
+    fraction of its algorithmic bytes per step, counting every transform's input
+    read and output written once: periodic 2R + 4H, advected 8R + 12H."""
     import numpy as np
     import smectic3d_b200 as S
     peak, _ = peaks()
