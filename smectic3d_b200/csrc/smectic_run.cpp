@@ -26,6 +26,7 @@ namespace {
 struct Opts {
   int n = 64, nw = 16, l1_every = 100, save_every = 100, surface_every = 0, amp_nw = 0;
   double sub_sigma = 0.0, sub_z0 = 1e-4;
+  bool alternate = false;
   long long max_steps = -1;
   double dt = 0.001, eps = -0.7, beta = 2.0, gamma = 1.0, alpha = 1.0, q0 = 1.0, eta = 1.0, rho = 1.0, w_mid = 0.0;
   double l1_limit = 1e-6;
@@ -43,7 +44,9 @@ void usage() {
       "  --surface-every m  every m-th L1 evaluation, end the block with the surface pass and append\n"
       "                     surfPsi.dat, velSurf.dat, curvH.dat, curvK.dat (Neumann: all columns, keeping\n"
       "                     the last value where no crossing is found; periodic: surfTrack, crossings only)\n"
-      "  --amp-nw Nw        at the end, write the local-amplitude map psiAvg.dat (morphSurfAmp)");
+      "  --amp-nw Nw        at the end, write the local-amplitude map psiAvg.dat (morphSurfAmp)\n"
+      "  --alternate        saves alternate between psi.dat and psiB.dat and append the y = N/2\n"
+      "                     slice of psi to psiMid.dat (cosNoAdvMorphCurv.cpp:980-1045)");
 }
 
 bool parse(int argc, char** argv, Opts& o) {
@@ -83,6 +86,7 @@ bool parse(int argc, char** argv, Opts& o) {
     else if (a == "--sub-z0") o.sub_z0 = std::atof(need("--sub-z0"));
     else if (a == "--surface-every") o.surface_every = std::atoi(need("--surface-every"));
     else if (a == "--amp-nw") o.amp_nw = std::atoi(need("--amp-nw"));
+    else if (a == "--alternate") o.alternate = true;
     else {
       std::fprintf(stderr, "unknown option %s\n", a.c_str());
       usage();
@@ -196,6 +200,8 @@ int main(int argc, char** argv) {
   double l1 = 1.0;
   long long steps = 0;
   int count_save = 0, count_surf = 0;
+  long long saves = 0;
+  if (o.alternate) std::ofstream(o.out + "/psiMid.dat").close();
   while (l1 > o.l1_limit && (o.max_steps < 0 || steps < o.max_steps)) {
     const int k = o.max_steps < 0 ? o.l1_every : int(std::min<long long>(o.l1_every, o.max_steps - steps));
     const bool surf = o.surface_every > 0 && k == o.l1_every && ++count_surf == o.surface_every;
@@ -239,7 +245,16 @@ int main(int argc, char** argv) {
     std::ofstream(o.out + "/L1.dat", std::ios_base::app) << l1 << "\n";
     if (++count_save == o.save_every) {
       sh_get_psi(h, psi.data(), SH_LAYOUT_DENSE);
-      write_psi(o.out + "/psi.dat", psi);
+      if (o.alternate) {
+        // psiMid.dat: the y = N/2 plane, i then k, "\n" separated; psi.dat and psiB.dat in turn
+        std::ofstream mid(o.out + "/psiMid.dat", std::ios_base::app);
+        for (int i = 0; i < o.n; ++i)
+          for (int k = 0; k < o.n; ++k) mid << psi[(size_t(i) * o.n + o.n / 2) * o.n + k] << "\n";
+        write_psi(o.out + (saves % 2 == 0 ? "/psi.dat" : "/psiB.dat"), psi);
+        ++saves;
+      } else {
+        write_psi(o.out + "/psi.dat", psi);
+      }
       count_save = 0;
     }
   }

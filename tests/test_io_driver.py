@@ -83,13 +83,18 @@ def test_driver_neumann_surface_and_amplitude(tmp_path):
     n = 32
     r = subprocess.run([DRIVER, "--n", str(n), "--nw", "8", "--dt", "0.05", "--eps", "-0.7", "--ic", "hyperboloid",
                         "--boundary", "neumann", "--sub-sigma", "0.3", "--sub-z0", "1.5", "--l1-every", "5",
-                        "--surface-every", "2", "--max-steps", "20", "--amp-nw", "8", "--out", str(tmp_path)],
+                        "--surface-every", "2", "--max-steps", "20", "--amp-nw", "8", "--alternate",
+                        "--save-every", "1", "--out", str(tmp_path)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     z = np.loadtxt(tmp_path / "surfPsi.dat")
     assert z.size == 2 * n * n  # two saves (blocks 2 and 4), every column
     assert np.isfinite(np.loadtxt(tmp_path / "curvH.dat")).all()
+    mid = np.loadtxt(tmp_path / "psiMid.dat")
+    assert mid.size == 4 * n * n  # one y = N/2 slice per save, four saves
+    assert (tmp_path / "psiB.dat").exists()
     psi = sio.read_psi_text(tmp_path / "psi.dat", n)
+    assert np.allclose(mid[-n * n:].reshape(n, n), psi[:, n // 2, :], atol=1e-5)  # last save = final state
     amp = sio.read_psi_text(tmp_path / "psiAvg.dat", n)
     from oracle import sh_oracle as O
     ref = O.local_amplitude(psi, 2 * np.pi / 8, 8)
