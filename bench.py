@@ -251,19 +251,22 @@ def run_ours(args, rank, world, local_rank, dist):
 
     # ---- accuracy of the FP32 path after 100 steps (the north-star check),
     # on the workload's IC and on the non-decaying reference-amplitude lamellae
-    acc100 = {}
+    acc100, energy_rel = {}, {}
     for label, ic0 in (("workload_ic", psi0),
                        ("lamellae_amp1.3", S.ic.undulated_lamellae(n, p32.dx, amp=1.3, seed=rank)
                         if batch == 1 else None)):
         if ic0 is None:
             continue
-        outs = {}
+        outs, ens = {}, {}
         for pr in ("fp32", "fp64"):
             with S.Solver(params_for(args.workload, pr)) as sv:
                 sv.set_psi(ic0)
                 sv.step(100)
                 outs[pr] = sv.get_psi()
+                ens[pr] = np.asarray(sv.energy(), dtype=np.float64)
         acc100[label] = float(np.linalg.norm(outs["fp32"] - outs["fp64"]) / np.linalg.norm(outs["fp64"]))
+        # energy of the FP32 state (FP64 sums) against the FP64 state's
+        energy_rel[label] = float(np.max(np.abs(ens["fp32"] - ens["fp64"]) / np.abs(ens["fp64"])))
 
     # ---- per-pass device times (roofline of the dominant kernel) -----------
     nprof = max(10, min(200, k // 10))
@@ -328,7 +331,8 @@ def run_ours(args, rank, world, local_rank, dist):
         "other_precision": {"precision": other, "value": world * k / (ms64 / 1e3), "ms_per_step": ms64 / k,
                             "speedup_fp32_over_fp64": (ms64 / ms) if prec == "fp32" else (ms / ms64),
                             "rel_err_fp32_vs_fp64": rel_err, "after_steps": w + k,
-                            "rel_err_fp32_vs_fp64_after_100_steps": acc100},
+                            "rel_err_fp32_vs_fp64_after_100_steps": acc100,
+                            "energy_rel_err_fp32_vs_fp64_after_100_steps": energy_rel},
         "adjoint_forward_ratio": adj["backward_over_forward"] if adj else None,
         "adjoint": adj,
         "other_configs": others,
