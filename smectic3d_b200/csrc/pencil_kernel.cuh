@@ -215,6 +215,7 @@ pencil_kernel(PencilArgs<T> a) {
   double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::red_off(MODE));
   const TwTables<T> tw =
       stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::tw_off(MODE)), a.tw, threadIdx.x, Cfg::THREADS);
+  grid_dependency_wait();
 
   const int f0 = blockIdx.x * TK;
   const int rep = blockIdx.y;

@@ -685,6 +685,7 @@ plane_kernel(PlaneArgs<T> a) {
     }
     cluster_arrive<CL>();  // matched by the wait of the first exchange
   }
+  grid_dependency_wait();
   const int x = blockIdx.x / CL;
   const int rep = blockIdx.y;
   const int line = threadIdx.x / G, t = threadIdx.x % G;

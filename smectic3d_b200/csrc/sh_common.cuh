@@ -34,6 +34,12 @@ __device__ __forceinline__ void mbar_wait_bounded(uint64_t* mbar, uint32_t parit
   }
 }
 
+// Programmatic dependent launch: the step kernels are launched so that they
+// may start while the previous kernel of the stream drains; everything before
+// this wait touches only data no kernel of the step writes (twiddles,
+// wavenumbers, shared memory set-up).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 enum NonlinKind : int { kQuintic = 0, kQuadCubic = 1 };
 enum SchemeKind : int { kCNAB2 = 0, kIMEXEuler = 1 };
 enum PassFlags : int {

@@ -2,6 +2,7 @@
 // plane and pencil passes of each time step.
 #pragma once
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -102,6 +103,8 @@ struct Solver final : SolverBase {
   using PC = PlaneCfg<T, N, CL, DCT>;
   using QC = PencilCfg<T, N, DCT>;
   static constexpr int FP = PC::FP;
+  // step kernels may start while the previous kernel drains (SMECTIC_B200_NO_PDL=1: off)
+  bool use_pdl = getenv("SMECTIC_B200_NO_PDL") == nullptr;
 
   cplx<T>* W = nullptr;
   cplx<T>* P = nullptr;
@@ -285,13 +288,22 @@ struct Solver final : SolverBase {
     cfg.blockDim = dim3(PC::THREADS, 1, 1);
     cfg.dynamicSmemBytes = PC::SMEM;
     cfg.stream = stream;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = CL;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
+    cudaLaunchAttribute attr[2];
+    unsigned na = 0;
+    if (CL > 1) {
+      attr[na].id = cudaLaunchAttributeClusterDimension;
+      attr[na].val.clusterDim.x = CL;
+      attr[na].val.clusterDim.y = 1;
+      attr[na].val.clusterDim.z = 1;
+      ++na;
+    }
+    if (use_pdl) {
+      attr[na].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[na].val.programmaticStreamSerializationAllowed = 1;
+      ++na;
+    }
     cfg.attrs = attr;
-    cfg.numAttrs = CL > 1 ? 1 : 0;
+    cfg.numAttrs = na;
     SHB_CUDA(cudaLaunchKernelEx(&cfg, plane_fn<MODE>(), a));
     ++launches;
     return SH_OK;
@@ -299,8 +311,17 @@ struct Solver final : SolverBase {
 
   template <int MODE>
   int launch_pencil(const PencilArgs<T>& a) {
-    pencil_fn<MODE>()<<<dim3(QC::TILES, p.batch, 1), QC::THREADS, QC::smem(MODE), stream>>>(a);
-    SHB_CUDA(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(QC::TILES, p.batch, 1);
+    cfg.blockDim = dim3(QC::THREADS, 1, 1);
+    cfg.dynamicSmemBytes = QC::smem(MODE);
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = use_pdl ? 1 : 0;
+    SHB_CUDA(cudaLaunchKernelEx(&cfg, pencil_fn<MODE>(), a));
     ++launches;
     return SH_OK;
   }
