@@ -19,6 +19,11 @@
 
 namespace shb {
 
+// warps per SM the FP32 step kernels are register-budgeted for
+#ifndef SHB_STEP_WARPS
+#define SHB_STEP_WARPS 24
+#endif
+
 enum PencilMode : int {
   kPencilStep = 0,
   kPencilInit = 1,
@@ -58,10 +63,13 @@ struct PencilCfg {
   static constexpr size_t tw_off(int mode) { return SET_BYTES * pencil_sets(mode); }
   static constexpr size_t red_off(int mode) { return tw_off(mode) + size_t(tw_total<N>()) * sizeof(cplx<T>); }
   static constexpr size_t smem(int mode) { return red_off(mode) + 64 * sizeof(double); }
-  // The FP32 step runs three 256-thread CTAs per SM (at most 85 registers a
-  // thread); every other launch leaves the register budget to ptxas (0).
+  // The FP32 step asks ptxas for a register budget that keeps 24 warps per SM
+  // resident (three 256-thread CTAs at 256^3, twelve 64-thread CTAs at 64^3);
+  // every other launch leaves the register budget to ptxas (0).
   static constexpr int min_blocks(int mode) {
-    return (sizeof(T) == 4 && mode == kPencilStep && THREADS == 256) ? 3 : 0;
+    return (sizeof(T) == 4 && mode == kPencilStep && THREADS <= 256 && SHB_STEP_WARPS * 32 / THREADS >= 2)
+               ? SHB_STEP_WARPS * 32 / THREADS
+               : 0;
   }
   static_assert(FP % TK == 0, "tile must divide the plane");
   static_assert(THREADS % 32 == 0, "pencil CTA must be whole warps");

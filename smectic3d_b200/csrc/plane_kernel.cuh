@@ -78,14 +78,22 @@ struct PlaneCfg {
   static constexpr size_t RED_OFF = MB_OFF + 16;
   static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
   static constexpr bool fits = SMEM <= 227 * 1024;  // per-CTA shared memory limit of sm_100
-  // Three resident CTAs need SMEM <= (228 KB - 3 x 1 KB reserved) / 3 and at
-  // most 85 registers a thread; ptxas is asked for the latter only where the
-  // former holds (FP32 clusters of 256-thread CTAs).
+  // FP32: ptxas is asked for a register budget that keeps SHB_STEP_WARPS warps
+  // per SM resident, where that many CTAs also fit the 228 KB of shared memory
+  // (1 KB reserved per CTA): three 256-thread CTAs in clusters at 256^3, six
+  // 128-thread CTAs at 64^3.
 #ifndef SHB_PLANE_THREE
 #define SHB_PLANE_THREE 1
 #endif
+#ifndef SHB_STEP_WARPS
+#define SHB_STEP_WARPS 24
+#endif
+  static constexpr int MIN_BLOCKS_RAW = THREADS <= 256 ? SHB_STEP_WARPS * 32 / THREADS : 0;
   static constexpr int MIN_BLOCKS =
-      (SHB_PLANE_THREE && sizeof(T) == 4 && CL > 1 && THREADS == 256 && SMEM <= 76800) ? 3 : 0;
+      (SHB_PLANE_THREE && sizeof(T) == 4 && MIN_BLOCKS_RAW >= 2 &&
+       (SMEM + 1024) * MIN_BLOCKS_RAW <= 233472)
+          ? MIN_BLOCKS_RAW
+          : 0;
   // kPlaneAdvN keeps an accumulator beside the transform registers: no cap
   static constexpr int min_blocks(int mode) { return mode == kPlaneAdvN ? 0 : MIN_BLOCKS; }
   static_assert(THREADS % 32 == 0, "plane CTA must be whole warps");
