@@ -23,6 +23,9 @@ namespace shb {
 #ifndef SHB_STEP_WARPS
 #define SHB_STEP_WARPS 24
 #endif
+#ifndef SHB_STEP_WARPS_F64
+#define SHB_STEP_WARPS_F64 16
+#endif
 
 enum PencilMode : int {
   kPencilStep = 0,
@@ -63,13 +66,15 @@ struct PencilCfg {
   static constexpr size_t tw_off(int mode) { return SET_BYTES * pencil_sets(mode); }
   static constexpr size_t red_off(int mode) { return tw_off(mode) + size_t(tw_total<N>()) * sizeof(cplx<T>); }
   static constexpr size_t smem(int mode) { return red_off(mode) + 64 * sizeof(double); }
-  // The FP32 step asks ptxas for a register budget that keeps 24 warps per SM
-  // resident (three 256-thread CTAs at 256^3, twelve 64-thread CTAs at 64^3);
-  // every other launch leaves the register budget to ptxas (0).
+  // The step asks ptxas for a register budget that keeps SHB_STEP_WARPS warps
+  // per SM resident in FP32 (three 256-thread CTAs at 256^3, twelve 64-thread
+  // CTAs at 64^3) and SHB_STEP_WARPS_F64 in FP64 at N <= 128; every other
+  // launch leaves the register budget to ptxas (0).
+  // FP64 holds twice the registers per value: only its small CTAs (N <= 128) get a budget
+  static constexpr int step_warps() { return sizeof(T) == 4 ? SHB_STEP_WARPS : (THREADS <= 64 ? SHB_STEP_WARPS_F64 : 0); }
   static constexpr int min_blocks(int mode) {
-    return (sizeof(T) == 4 && mode == kPencilStep && THREADS <= 256 && SHB_STEP_WARPS * 32 / THREADS >= 2)
-               ? SHB_STEP_WARPS * 32 / THREADS
-               : 0;
+    return (mode == kPencilStep && THREADS <= 256 && step_warps() * 32 / THREADS >= 2) ? step_warps() * 32 / THREADS
+                                                                                      : 0;
   }
   static_assert(FP % TK == 0, "tile must divide the plane");
   static_assert(THREADS % 32 == 0, "pencil CTA must be whole warps");
