@@ -149,10 +149,8 @@ int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes);
  * No counterpart in the reference: it is the monitor of sh_l1 (the
  * reference's L1 of periodicFFT/pf3d.cpp:489-509, evaluated on caller
  * buffers) for callers that must not let a library allocate. Examples: a host
- * that manages all device memory through its own pool, code running while a
- * stream is captured into a CUDA graph (cudaMalloc/cudaFree are not allowed
- * there), and real-time loops that cannot take the implicit device
- * synchronisation of cudaMalloc/cudaFree.
+ * that manages all device memory through its own pool, and real-time loops
+ * that cannot take the implicit device synchronisation of cudaMalloc/cudaFree.
  *
  * dev_psi_new, dev_psi_old: batch*n3 doubles each on the current device.
  * dev_out: batch doubles on the current device; receives

@@ -6,8 +6,6 @@
 // sh_create allocates. This variant keeps those partial sums in a fixed
 // file-scope device array instead. Some callers cannot let a library allocate:
 //  - a host that owns device memory through its own pool allocator;
-//  - a code path running while a stream is being captured into a CUDA graph,
-//    where cudaMalloc and cudaFree are not allowed;
 //  - a real-time loop that cannot afford the implicit device synchronisation
 //    of cudaMalloc/cudaFree.
 // Such a caller passes its own input fields and output buffer, and the call

@@ -3,7 +3,6 @@ handle-based monitor behind sh_l1.
 
 sh_l1_noalloc is for callers that cannot let a library call cudaMalloc:
  - hosts that own all device memory through their own pool;
- - code that runs while a stream is being captured into a CUDA graph;
  - real-time loops that cannot take the implicit synchronisation of an
    allocation.
 This test therefore owns every device buffer it passes. It checks the result
