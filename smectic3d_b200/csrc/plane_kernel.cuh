@@ -115,7 +115,7 @@ struct PlaneArgs {
   // real-field modes: wavenumber table, multiplier, real inputs / output
   const T* q;
   int mult;
-  const T* real_in[7];
+  const T* real_in[4];  // adjoint: [1] psi; stress: [0] L psi; advected N: [0] psi, [1..3] grad psi
   T* real_out;
   // kPlaneInvReal: optional second partial, added after its own multiplier
   const cplx<T>* src2;
