@@ -112,6 +112,31 @@ def neumann_substrate():
     return _pack(p, psi0=psi0, psi=o.psi, steps=10)
 
 
+def _sub(psi):
+    """Compact record of a 64^3 state: every 4th point per axis and two global sums."""
+    return {"psi_sub": psi[::4, ::4, ::4].copy(), "sum_sq": float(np.sum(psi * psi)),
+            "sum_abs": float(np.sum(np.abs(psi)))}
+
+
+def periodic_plain_64():
+    # the initial condition is regenerated by the test from (ic, seed): only outputs are stored
+    n = 64
+    p = O.Params(n=n, dt=0.05, eps=-0.7)
+    psi0 = ic.noise(n, 11, 0.2) + 1.3 * np.cos(np.arange(n) * p.dx)[None, None, :]
+    o = O.PeriodicOracle(psi0, p)
+    o.run(20)
+    return _pack(p, ic_kind="noise11+lamellae1.3", steps=20, **_sub(o.psi))
+
+
+def neumann_hyperboloid_64():
+    n = 64
+    p = O.Params(n=n, dt=0.05, eps=-0.7)
+    psi0 = ic.hyperboloid(n, p.dx, r0_cells=12.0, seed=12)
+    o = O.NeumannOracle(psi0, p)
+    o.run(20)
+    return _pack(p, ic_kind="hyperboloid12", steps=20, **_sub(o.psi))
+
+
 CASES = {
     "periodic_plain_16": periodic_plain,
     "periodic_lamellae_32": periodic_lamellae_ref_ic,
@@ -121,6 +146,8 @@ CASES = {
     "neumann_l1_32": neumann_l1,
     "periodic_advected_16": periodic_advected,
     "neumann_substrate_16": neumann_substrate,
+    "periodic_plain_64": periodic_plain_64,
+    "neumann_hyperboloid_64": neumann_hyperboloid_64,
 }
 
 

@@ -276,3 +276,16 @@ def test_local_amplitude_of_uniform_lamellae_is_one():
     psi = np.broadcast_to(1.3 * np.cos(np.arange(n) * dx + 0.4)[None, None, :], (n, n, n))
     m = O.local_amplitude(psi, dx, 8)
     assert np.abs(m[4:-4, 4:-4, 4:-4] - 1).max() < 1e-12
+
+
+def test_golden_64_regenerates_from_its_seed():
+    """The compact 64^3 golden vectors store outputs only: their seeded initial
+    conditions must regenerate to the same oracle run."""
+    import os
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "neumann_hyperboloid_64.npz"))
+    from smectic3d_b200 import ic
+    n = 64
+    p = O.Params(n=n, dt=float(d["param_dt"]), eps=float(d["param_eps"]))
+    o = O.NeumannOracle(ic.hyperboloid(n, p.dx, r0_cells=12.0, seed=12), p)
+    o.run(int(d["steps"]))
+    assert np.allclose(o.psi[::4, ::4, ::4], d["psi_sub"], rtol=0, atol=1e-13)

@@ -71,6 +71,30 @@ def test_golden_vectors(name, boundary, prec):
             assert abs(l1[0] - float(d["l1"])) <= (1e-9 if prec == "fp64" else 1e-3) * abs(float(d["l1"]))
 
 
+def _golden64_ic(kind, n, dx):
+    if kind == "noise11+lamellae1.3":
+        return S.ic.noise(n, 11, 0.2) + 1.3 * np.cos(np.arange(n) * dx)[None, None, :]
+    if kind == "hyperboloid12":
+        return S.ic.hyperboloid(n, dx, r0_cells=12.0, seed=12)
+    raise ValueError(kind)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("name,boundary", [("periodic_plain_64", "periodic"), ("neumann_hyperboloid_64", "neumann")])
+def test_golden_vectors_64(name, boundary, prec):
+    """64^3 golden states, stored compactly (every 4th point per axis and two global sums);
+    the seeded initial condition is regenerated here."""
+    d, kw = golden(name)
+    p = S.Params(boundary=boundary, precision=prec, **{k: v for k, v in kw.items() if k in S.Params.__dataclass_fields__})
+    with S.Solver(p) as s:
+        s.set_psi(_golden64_ic(str(d["ic_kind"]), p.n, p.dx))
+        s.step(int(d["steps"]))
+        psi = s.get_psi()
+    assert rel(psi[::4, ::4, ::4], d["psi_sub"]) <= TOL[prec]
+    assert abs(float(np.sum(psi * psi)) - float(d["sum_sq"])) <= TOL[prec] * float(d["sum_sq"])
+    assert abs(float(np.sum(np.abs(psi))) - float(d["sum_abs"])) <= TOL[prec] * float(d["sum_abs"])
+
+
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("boundary", ["periodic", "neumann"])
 @pytest.mark.parametrize("n", [32, 64, 128])
