@@ -183,22 +183,29 @@ int sh_create(const sh_params* p, sh_handle** out) {
     h->s = nullptr;
     return SH_ECUDA;
   };
+  {
+    const char* fa = getenv("SMECTIC_B200_TEST_FAIL_ALLOC");
+    alloc_fail_countdown() = fa ? atoi(fa) : 0;
+  }
+  struct Disarm {
+    ~Disarm() { alloc_fail_countdown() = 0; }
+  } disarm;
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking)) != cudaSuccess) {
     s->err = cudaGetErrorString(e);
     return bad("stream");
   }
-  if ((e = cudaMalloc(&s->d_flag, 2 * sizeof(int))) != cudaSuccess ||
-      (e = cudaMalloc(&s->d_psi, n3 * p->batch * sizeof(double))) != cudaSuccess ||
-      (e = cudaMalloc(&s->d_eps, p->batch * sizeof(double))) != cudaSuccess ||
-      (e = cudaMalloc(&s->d_scalar, p->batch * sizeof(double))) != cudaSuccess) {
+  if ((e = dev_malloc(&s->d_flag, 2 * sizeof(int))) != cudaSuccess ||
+      (e = dev_malloc(&s->d_psi, n3 * p->batch * sizeof(double))) != cudaSuccess ||
+      (e = dev_malloc(&s->d_eps, p->batch * sizeof(double))) != cudaSuccess ||
+      (e = dev_malloc(&s->d_scalar, p->batch * sizeof(double))) != cudaSuccess) {
     s->err = cudaGetErrorString(e);
     delete s;
     h->s = nullptr;
     g_err = std::string("device allocation: ") + cudaGetErrorString(e);
     return SH_ENOMEM;
   }
-  if (p->l1_interval > 0 && (e = cudaMalloc(&s->d_stash, n3 * p->batch * sizeof(double))) != cudaSuccess) {
+  if (p->l1_interval > 0 && (e = dev_malloc(&s->d_stash, n3 * p->batch * sizeof(double))) != cudaSuccess) {
     delete s;
     h->s = nullptr;
     g_err = std::string("device allocation: ") + cudaGetErrorString(e);
@@ -298,7 +305,7 @@ int sh_local_amplitude(sh_handle* h, int nw, double* out) {
   if (rc) return rc;
   const size_t bytes = s->n3() * s->p.batch * sizeof(double);
   for (auto& b : s->d_amp)
-    if (!b) API_CUDA(h, cudaMalloc(&b, bytes));
+    if (!b) API_CUDA(h, dev_malloc(&b, bytes));
   const dim3 lines((unsigned)((size_t(n) * n + 255) / 256), s->p.batch);
   const double dx = s->p.dx;
   // psi^2 -> x window -> y window -> z window (morphSurfAmp.cpp:1076-1107)

@@ -14,6 +14,27 @@
 
 namespace shb {
 
+// Device allocations of the library go through here.  Test hook: while the
+// countdown is armed (only inside sh_create, from SMECTIC_B200_TEST_FAIL_ALLOC=k),
+// the k-th allocation fails as out of memory, which exercises the clean-up and
+// SH_ENOMEM paths without exhausting the GPU.
+inline int& alloc_fail_countdown() {
+  static thread_local int n = 0;
+  return n;
+}
+inline cudaError_t dev_malloc(void** ptr, size_t bytes) {
+  int& c = alloc_fail_countdown();
+  if (c > 0 && --c == 0) {
+    *ptr = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(ptr, bytes);
+}
+template <class P>
+inline cudaError_t dev_malloc(P** ptr, size_t bytes) {
+  return dev_malloc(reinterpret_cast<void**>(ptr), bytes);
+}
+
 #define SHB_CUDA(expr)                                                        \
   do {                                                                        \
     cudaError_t e_ = (expr);                                                  \
@@ -208,18 +229,18 @@ struct Solver final : SolverBase {
 
   int setup() override {
     const size_t fe = field_elems();
-    SHB_CUDA(cudaMalloc(&W, fe * sizeof(cplx<T>)));
-    SHB_CUDA(cudaMalloc(&P, fe * sizeof(cplx<T>)));
-    SHB_CUDA(cudaMalloc(&Nt, fe * sizeof(cplx<T>)));
+    SHB_CUDA(dev_malloc(&W, fe * sizeof(cplx<T>)));
+    SHB_CUDA(dev_malloc(&P, fe * sizeof(cplx<T>)));
+    SHB_CUDA(dev_malloc(&Nt, fe * sizeof(cplx<T>)));
     if (p.advection) {
       if constexpr (DCT) {
         err = "advection is defined for the periodic boundary only";
         return SH_EINVAL;
       } else {
-        SHB_CUDA(cudaMalloc(&Px, fe * sizeof(cplx<T>)));
-        SHB_CUDA(cudaMalloc(&PSH, fe * sizeof(cplx<T>)));
-        for (auto& p3 : S3) SHB_CUDA(cudaMalloc(&p3, fe * sizeof(cplx<T>)));
-        for (auto& r : R) SHB_CUDA(cudaMalloc(&r, size_t(p.batch) * N * N * N * sizeof(T)));
+        SHB_CUDA(dev_malloc(&Px, fe * sizeof(cplx<T>)));
+        SHB_CUDA(dev_malloc(&PSH, fe * sizeof(cplx<T>)));
+        for (auto& p3 : S3) SHB_CUDA(dev_malloc(&p3, fe * sizeof(cplx<T>)));
+        for (auto& r : R) SHB_CUDA(dev_malloc(&r, size_t(p.batch) * N * N * N * sizeof(T)));
       }
     }
     if (p.sub_sigma != 0.0) {
@@ -236,16 +257,16 @@ struct Solver final : SolverBase {
           hw.push_back(T(w));
         }
         kwall = int(hw.size());
-        SHB_CUDA(cudaMalloc(&Pxx, fe * sizeof(cplx<T>)));
-        SHB_CUDA(cudaMalloc(&Lp, size_t(p.batch) * N * N * kwall * sizeof(T)));
-        SHB_CUDA(cudaMalloc(&d_wall, kwall * sizeof(T)));
+        SHB_CUDA(dev_malloc(&Pxx, fe * sizeof(cplx<T>)));
+        SHB_CUDA(dev_malloc(&Lp, size_t(p.batch) * N * N * kwall * sizeof(T)));
+        SHB_CUDA(dev_malloc(&d_wall, kwall * sizeof(T)));
         SHB_CUDA(cudaMemcpy(d_wall, hw.data(), kwall * sizeof(T), cudaMemcpyHostToDevice));
       }
     }
-    SHB_CUDA(cudaMalloc(&tw, tw_total<N>() * sizeof(cplx<T>)));
-    SHB_CUDA(cudaMalloc(&q, N * sizeof(T)));
-    SHB_CUDA(cudaMalloc(&d_red_plane, size_t(p.batch) * N * CL * 3 * sizeof(double)));
-    SHB_CUDA(cudaMalloc(&d_red_spec, size_t(p.batch) * QC::TILES * sizeof(double)));
+    SHB_CUDA(dev_malloc(&tw, tw_total<N>() * sizeof(cplx<T>)));
+    SHB_CUDA(dev_malloc(&q, N * sizeof(T)));
+    SHB_CUDA(dev_malloc(&d_red_plane, size_t(p.batch) * N * CL * 3 * sizeof(double)));
+    SHB_CUDA(dev_malloc(&d_red_spec, size_t(p.batch) * QC::TILES * sizeof(double)));
     std::vector<cplx<T>> htw;
     host_twiddles<T, N>(htw);
     std::vector<T> hq(N);
@@ -461,7 +482,7 @@ struct Solver final : SolverBase {
     if (trace && n > trace_cap) {
       cudaFree(d_trace);
       d_trace = nullptr;
-      SHB_CUDA(cudaMalloc(&d_trace, size_t(n) * p.batch * sizeof(double)));
+      SHB_CUDA(dev_malloc(&d_trace, size_t(n) * p.batch * sizeof(double)));
       trace_cap = n;
     }
     for (int s = 0; s < n; ++s) {
@@ -701,7 +722,7 @@ struct Solver final : SolverBase {
         cudaFree(bf.ck);
         bf.ck = nullptr;
         bf.nseg = 0;
-        ADJ_CUDA(cudaMalloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
+        ADJ_CUDA(dev_malloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
         bf.nseg = nseg;
       }
       if (bf.k < K) {
@@ -710,16 +731,16 @@ struct Solver final : SolverBase {
         bf.hs = nullptr;
         bf.hr = nullptr;
         bf.k = 0;
-        ADJ_CUDA(cudaMalloc(&bf.hs, size_t(K + 1) * fe * sizeof(cplx<T>)));
-        ADJ_CUDA(cudaMalloc(&bf.hr, size_t(K + 1) * nr * sizeof(T)));
+        ADJ_CUDA(dev_malloc(&bf.hs, size_t(K + 1) * fe * sizeof(cplx<T>)));
+        ADJ_CUDA(dev_malloc(&bf.hr, size_t(K + 1) * nr * sizeof(T)));
         bf.k = K;
       }
       if (!bf.lam) {
-        ADJ_CUDA(cudaMalloc(&bf.lam, fe * sizeof(cplx<T>)));
-        ADJ_CUDA(cudaMalloc(&bf.gp, fe * sizeof(cplx<T>)));
-        ADJ_CUDA(cudaMalloc(&bf.mp, fe * sizeof(cplx<T>)));
-        ADJ_CUDA(cudaMalloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
-        ADJ_CUDA(cudaMalloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
+        ADJ_CUDA(dev_malloc(&bf.lam, fe * sizeof(cplx<T>)));
+        ADJ_CUDA(dev_malloc(&bf.gp, fe * sizeof(cplx<T>)));
+        ADJ_CUDA(dev_malloc(&bf.mp, fe * sizeof(cplx<T>)));
+        ADJ_CUDA(dev_malloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
+        ADJ_CUDA(dev_malloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
       }
       ADJ_CUDA(cudaMemsetAsync(bf.red, 0, size_t(p.batch) * QC::TILES * 2 * sizeof(double), stream));
       const size_t fb = fe * sizeof(cplx<T>);
@@ -831,10 +852,10 @@ struct Solver final : SolverBase {
       int rc;
       const size_t nr = size_t(p.batch) * N * N * N, nc = size_t(p.batch) * N * N;
       if (!CR[0]) {
-        for (auto& r : CR) SHB_CUDA(cudaMalloc(&r, nr * sizeof(T)));
-        SHB_CUDA(cudaMalloc(&Psc, field_elems() * sizeof(cplx<T>)));
-        SHB_CUDA(cudaMalloc(&d_zout, nc * sizeof(int)));
-        for (auto& d : d_surf) SHB_CUDA(cudaMalloc(&d, nc * sizeof(double)));
+        for (auto& r : CR) SHB_CUDA(dev_malloc(&r, nr * sizeof(T)));
+        SHB_CUDA(dev_malloc(&Psc, field_elems() * sizeof(cplx<T>)));
+        SHB_CUDA(dev_malloc(&d_zout, nc * sizeof(int)));
+        for (auto& d : d_surf) SHB_CUDA(dev_malloc(&d, nc * sizeof(double)));
       }
       // psi, psi_yy, psi_zz from the partial of psi; psi_xx and L psi through an x multiplier
       const int mult[3] = {kMulNone, kMulNegQy2, kMulNegQz2};
@@ -893,9 +914,9 @@ struct Solver final : SolverBase {
       int rc;
       const size_t nr = size_t(p.batch) * N * N * N, nc = size_t(p.batch) * N * N;
       if (!SR[0]) {
-        for (auto& r : SR) SHB_CUDA(cudaMalloc(&r, nr * sizeof(T)));
-        SHB_CUDA(cudaMalloc(&d_zout, nc * sizeof(int)));
-        for (auto& d : d_surf) SHB_CUDA(cudaMalloc(&d, nc * sizeof(double)));
+        for (auto& r : SR) SHB_CUDA(dev_malloc(&r, nr * sizeof(T)));
+        SHB_CUDA(dev_malloc(&d_zout, nc * sizeof(int)));
+        for (auto& d : d_surf) SHB_CUDA(dev_malloc(&d, nc * sizeof(double)));
       }
       if (!real_fields_current && (rc = adv_nonlinear(0))) return rc;
       if (!u_real_current && (rc = velocity_real())) return rc;
