@@ -4,6 +4,8 @@
 #include <memory>
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "amplitude_kernel.cuh"
 #include "sh_solver.cuh"
 
@@ -14,6 +16,14 @@ struct sh_handle {
 };
 
 static thread_local std::string g_err;
+
+// NVTX range over one public call (named after the entry point), so that a
+// timeline profiler shows the library's calls; without a tool attached the
+// push and pop are no-ops.
+struct ApiRange {
+  explicit ApiRange(const char* name) { nvtxRangePushA(name); }
+  ~ApiRange() { nvtxRangePop(); }
+};
 
 namespace shb {
 void set_global_error(const std::string& msg) { g_err = msg; }
@@ -144,6 +154,7 @@ int sh_default_params(sh_params* p) {
 }
 
 int sh_create(const sh_params* p, sh_handle** out) {
+  ApiRange range_("sh_create");
   if (!p || !out) return fail(nullptr, SH_EINVAL, "null argument");
   *out = nullptr;
   if (!supported_n(p->n)) return fail(nullptr, SH_EUNSUPPORTED, "n must be one of 16, 32, 64, 128, 256, 512");
@@ -238,6 +249,7 @@ int sh_destroy(sh_handle* h) {
 }
 
 int sh_set_psi_device(sh_handle* h, const double* dev_psi) {
+  ApiRange range_("sh_set_psi_device");
   if (!h || !h->s || !dev_psi) return fail(h, SH_EINVAL, "null argument");
   SolverBase* s = h->s;
   if (dev_psi != s->d_psi)
@@ -248,6 +260,7 @@ int sh_set_psi_device(sh_handle* h, const double* dev_psi) {
 }
 
 int sh_set_psi(sh_handle* h, const double* host_psi, int layout) {
+  ApiRange range_("sh_set_psi");
   if (!h || !h->s || !host_psi) return fail(h, SH_EINVAL, "null argument");
   if (layout != SH_LAYOUT_DENSE && layout != SH_LAYOUT_PADDED) return fail(h, SH_EINVAL, "bad layout");
   SolverBase* s = h->s;
@@ -264,6 +277,7 @@ int sh_set_psi(sh_handle* h, const double* host_psi, int layout) {
 }
 
 int sh_get_psi_device(sh_handle* h, double* dev_psi) {
+  ApiRange range_("sh_get_psi_device");
   if (!h || !h->s || !dev_psi) return fail(h, SH_EINVAL, "null argument");
   SolverBase* s = h->s;
   if (!s->ready) return fail(h, SH_ESTATE, "psi was never set");
@@ -276,6 +290,7 @@ int sh_get_psi_device(sh_handle* h, double* dev_psi) {
 }
 
 int sh_get_psi(sh_handle* h, double* host_psi, int layout) {
+  ApiRange range_("sh_get_psi");
   if (!h || !h->s || !host_psi) return fail(h, SH_EINVAL, "null argument");
   if (layout != SH_LAYOUT_DENSE && layout != SH_LAYOUT_PADDED) return fail(h, SH_EINVAL, "bad layout");
   SolverBase* s = h->s;
@@ -296,6 +311,7 @@ int sh_get_psi(sh_handle* h, double* host_psi, int layout) {
 }
 
 int sh_local_amplitude(sh_handle* h, int nw, double* out) {
+  ApiRange range_("sh_local_amplitude");
   if (!h || !h->s || !out) return fail(h, SH_EINVAL, "null argument");
   SolverBase* s = h->s;
   if (!s->ready) return fail(h, SH_ESTATE, "psi was never set");
@@ -323,6 +339,7 @@ int sh_local_amplitude(sh_handle* h, int nw, double* out) {
 }
 
 int sh_step_async(sh_handle* h, int nsteps) {
+  ApiRange range_("sh_step_async");
   if (!h || !h->s) return fail(h, SH_EINVAL, "null handle");
   if (nsteps < 0) return fail(h, SH_EINVAL, "nsteps must be >= 0");
   if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
@@ -330,6 +347,7 @@ int sh_step_async(sh_handle* h, int nsteps) {
 }
 
 int sh_step(sh_handle* h, int nsteps) {
+  ApiRange range_("sh_step");
   int rc = sh_step_async(h, nsteps);
   if (rc) return rc;
   SolverBase* s = h->s;
@@ -351,6 +369,7 @@ int sh_step(sh_handle* h, int nsteps) {
 }
 
 int sh_run(sh_handle* h, const double* host_psi0, int nsteps, double* host_psi_out, int layout) {
+  ApiRange range_("sh_run");
   int rc = sh_set_psi(h, host_psi0, layout);
   if (rc) return rc;
   if ((rc = sh_step(h, nsteps))) return rc;
@@ -358,6 +377,7 @@ int sh_run(sh_handle* h, const double* host_psi0, int nsteps, double* host_psi_o
 }
 
 int sh_energy(sh_handle* h, double* out) {
+  ApiRange range_("sh_energy");
   if (!h || !h->s || !out) return fail(h, SH_EINVAL, "null argument");
   if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
   return h->s->energy_now(out);
@@ -384,6 +404,7 @@ int sh_l1(sh_handle* h, double* out, int* count) {
 }
 
 int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kgauss) {
+  ApiRange range_("sh_surface_step");
   if (!h || !h->s || !z || !vn || !hmean || !kgauss) return fail(h, SH_EINVAL, "null argument");
   if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
   return h->s->surface_step(z, vn, hmean, kgauss);
@@ -391,6 +412,7 @@ int sh_surface_step(sh_handle* h, int* z, double* vn, double* hmean, double* kga
 
 int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every, double* g_eps,
                double* g_q0, double* g_psi0) {
+  ApiRange range_("sh_adjoint");
   if (!h || !h->s || !psi0 || !dl_dpsi_t || !g_eps || !g_q0 || !g_psi0) return fail(h, SH_EINVAL, "null argument");
   int rc = h->s->adjoint(psi0, nsteps, dl_dpsi_t, ckpt_every, g_eps, g_q0, g_psi0);
   if (rc == SH_OK) h->s->ready = true;
@@ -398,6 +420,7 @@ int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dp
 }
 
 int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes) {
+  ApiRange range_("sh_checkpoint_save");
   if (!h || !h->s || !bytes) return fail(h, SH_EINVAL, "null argument");
   SolverBase* s = h->s;
   const size_t need = sizeof(sh_params) + sizeof(long long) + s->state_bytes();
@@ -415,6 +438,7 @@ int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes) {
 }
 
 int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes) {
+  ApiRange range_("sh_checkpoint_load");
   if (!h || !h->s || !buf) return fail(h, SH_EINVAL, "null argument");
   SolverBase* s = h->s;
   const size_t need = sizeof(sh_params) + sizeof(long long) + s->state_bytes();
@@ -445,6 +469,7 @@ int sh_host_free(void* p) {
 }
 
 int sh_profile_steps(sh_handle* h, int nsteps, double* ms_pencil, double* ms_plane) {
+  ApiRange range_("sh_profile_steps");
   if (!h || !h->s || !ms_pencil || !ms_plane) return fail(h, SH_EINVAL, "null argument");
   SolverBase* s = h->s;
   if (!s->ready) return fail(h, SH_ESTATE, "psi was never set");
