@@ -306,6 +306,7 @@ def run_ours(args, rank, world, local_rank, dist):
 
     adj = adjoint_ratio(args, torch) if args.adjoint_steps > 0 else None
     others = other_configs(torch) if (world == 1 and args.other_configs) else None
+    comparator = cufft_comparator(torch) if (world == 1 and args.other_configs) else None
 
     if rank != 0:
         return None
@@ -336,6 +337,7 @@ def run_ours(args, rank, world, local_rank, dist):
         "adjoint_forward_ratio": adj["backward_over_forward"] if adj else None,
         "adjoint": adj,
         "other_configs": others,
+        "cufft_comparator": comparator,
     }
     return line
 
@@ -437,6 +439,49 @@ def other_configs(torch, steps=200):
         "roofline_frac": b * plain / (peak * 1e9), "surface_columns_found": found,
         "timing": "host clock around 10-step blocks (each surface pass returns to the host)"}
     return out
+
+
+def cufft_comparator(torch, steps=100):
+    """Context only: the plain periodic CNAB2 step at 256^3 FP32 written with
+    torch.fft (cuFFT) and elementwise torch ops, unfused, beside this library's
+    own periodic 256^3 FP32 step.  Same algorithm (W-state CNAB2, quintic N);
+    both timed with CUDA events over ``steps`` steps."""
+    import numpy as np
+    import smectic3d_b200 as S
+    n, dt, eps, beta, gamma = 256, 0.05, -0.75, 2.0, 1.0
+    p = S.Params(n=n, precision="fp32", dt=dt, eps=eps)
+    dev = torch.device("cuda")
+    k = torch.fft.fftfreq(n, d=p.dx / (2 * np.pi), device=dev, dtype=torch.float32)
+    kz = torch.fft.rfftfreq(n, d=p.dx / (2 * np.pi), device=dev, dtype=torch.float32)
+    q2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
+    a_lin = eps - (q2 - 1.0) ** 2
+    c1, inv_c2 = 1 + 0.5 * dt * a_lin, 1.0 / (1 - 0.5 * dt * a_lin)
+    psi = torch.tensor(S.ic.noise(n, 0), dtype=torch.float32, device=dev)
+    nl = lambda x: beta * x ** 3 - gamma * x ** 5
+    w = c1 * torch.fft.rfftn(psi) - 0.5 * dt * torch.fft.rfftn(nl(psi))
+
+    def step(psi, w):
+        nh = torch.fft.rfftn(nl(psi))
+        ph = (w + 1.5 * dt * nh) * inv_c2
+        return torch.fft.irfftn(ph, s=(n, n, n)), c1 * ph - 0.5 * dt * nh
+
+    for _ in range(5):
+        psi, w = step(psi, w)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(steps):
+        psi, w = step(psi, w)
+    e1.record()
+    e1.synchronize()
+    torch_rate = steps / (e0.elapsed_time(e1) / 1e3)
+    with S.Solver(p) as s:
+        s.set_psi(S.ic.noise(n, 0))
+        s.step(10)
+        ours = steps / (timed_steps(s, steps, torch, None) / 1e3)
+    return {"what": "plain periodic CNAB2 step, 256^3 FP32: torch.fft (cuFFT) + torch elementwise, unfused, "
+                    "against this library's fused passes",
+            "torch_fft_steps_per_s": torch_rate, "ours_steps_per_s": ours, "ours_over_torch_fft": ours / torch_rate}
 
 
 # ---------------------------------------------------------------------------
