@@ -175,12 +175,17 @@ __device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, i
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   __syncthreads();     // every thread's send-block writes precede the copies
   cluster_wait<CL>();  // every peer has arrived: its receive blocks are free, its mbarriers initialised
-  if (threadIdx.x == 0) {
+  // thread d copies block d (a copy may complete on a peer's mbarrier before
+  // that peer's expect_tx: the phase completes only once both have happened)
+  if (threadIdx.x < CL) {
+    const int d = threadIdx.x;
     const uint32_t bytes = uint32_t(blk * sizeof(cplx<T>));
-    const uint32_t mb = smem_u32(&x.mbar[which]);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes * CL) : "memory");
+    if (d == 0) {
+      const uint32_t mb = smem_u32(&x.mbar[which]);
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes * CL) : "memory");
+    }
     const bool send = !(x.drop && rank == 0 && which == 0);
-    for (int d = 0; send && d < CL; ++d) {
+    if (send) {
       const uint32_t dst = dsmem_map(x.rb + size_t(rank) * blk, d);
       const uint32_t src = smem_u32(x.sb + size_t(d) * blk);
       const uint32_t rmb = dsmem_map(&x.mbar[which], d);
@@ -195,9 +200,11 @@ __device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, i
   x.phases ^= 1u << which;
 }
 
-// The send blocks may be rewritten once this CTA's outgoing copies read them.
+// The send blocks may be rewritten once this CTA's outgoing copies read them
+// (each of the first CL threads waits for the copy it issued).
+template <int CL>
 __device__ __forceinline__ void send_blocks_free() {
-  if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+  if (threadIdx.x < CL) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
   __syncthreads();
 }
 
@@ -409,7 +416,7 @@ struct PlaneOps {
   // inverse z transform of row pair ``line``; v slot holds psi(y0, z), psi(y0+1, z)
   static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], const cplx<T>* buf, const Xchg<T>& xs,
                                                      cplx<T>* L, int q, int t, const TwTables<T>& tw) {
-    if constexpr (Cfg::ALIAS) send_blocks_free();  // the scratch L overlays the outgoing send blocks
+    if constexpr (Cfg::ALIAS) send_blocks_free<CL>();  // the scratch L overlays the outgoing send blocks
     if constexpr (!DCT) {
       // Z = X_a + i X_b with Hermitian extension; slot 0 holds (X[0], X[N/2])
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
@@ -487,7 +494,7 @@ struct PlaneOps {
           }
         __syncthreads();
       } else {
-        send_blocks_free();
+        send_blocks_free<CL>();
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -526,7 +533,7 @@ struct PlaneOps {
           }
         __syncthreads();
       } else {
-        send_blocks_free();
+        send_blocks_free<CL>();
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -545,7 +552,7 @@ struct PlaneOps {
   // ---- column phase, forward direction ---------------------------------
   static __device__ void col_forward_store(cplx<T>* buf, const Xchg<T>& xs, cplx<T>* __restrict__ plane, int rank,
                                            const TwTables<T>& tw) {
-    if constexpr (Cfg::ALIAS) send_blocks_free();  // the scratch L overlays the outgoing send blocks
+    if constexpr (Cfg::ALIAS) send_blocks_free<CL>();  // the scratch L overlays the outgoing send blocks
     const int line = threadIdx.x / G, t = threadIdx.x % G;
     cplx<T>* L = buf + line * LS;
     cplx<T> v[E];
@@ -893,7 +900,7 @@ plane_kernel(PlaneArgs<T> a) {
   }
   if constexpr (CL > 1) {
     // outgoing copies must have finished reading this CTA's send blocks
-    if (threadIdx.x == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    if (threadIdx.x < CL) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
 }
 
