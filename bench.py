@@ -271,6 +271,7 @@ def run_ours(args, rank, world, local_rank, dist):
     # ---- per-pass device times (roofline of the dominant kernel) -----------
     nprof = max(10, min(200, k // 10))
     ms_pencil, ms_plane = s32.profile_steps(nprof)
+    residency = s32.residency()
     s32.close()
     ab = algorithmic_bytes(bnd, n, batch, prec)
     per = {"pencil": ms_pencil / nprof, "plane": ms_plane / nprof}
@@ -324,7 +325,7 @@ def run_ours(args, rank, world, local_rank, dist):
                      "algorithmic_bytes_per_launch": ab[dom], "avg_launch_ms": per[dom],
                      "traffic": (tr["bytes_per_launch"] if tr else None),
                      "step_frac": (ab["pencil"] + ab["plane"]) / (ms / k / 1e3) / 1e9 / peak,
-                     "pass_ms": per},
+                     "pass_ms": per, "residency": residency},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,

@@ -180,6 +180,15 @@ int sh_host_free(void* p);
  * the summed device milliseconds of the pencil (x) and plane (y,z) passes. */
 int sh_profile_steps(sh_handle* h, int nsteps, double* ms_pencil, double* ms_plane);
 
+/* Residency of the two step kernels on the handle's GPU, written to out[7]:
+ *   out[0] plane-pass CTAs per SM, out[1] plane clusters resident at once,
+ *   out[2] plane cluster size (CTAs), out[3] plane CTAs in one pass,
+ *   out[4] pencil-pass CTAs per SM, out[5] pencil CTAs in one pass,
+ *   out[6] SM count.
+ * A pass of G CTAs runs in G / (resident CTAs) waves; when that is not a
+ * whole number the last wave leaves SMs idle.  Allocates nothing. */
+int sh_residency(sh_handle* h, int* out);
+
 int sh_synchronize(sh_handle* h);
 void* sh_stream(sh_handle* h);               /* the handle's cudaStream_t */
 long long sh_steps_taken(sh_handle* h);

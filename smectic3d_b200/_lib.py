@@ -23,7 +23,7 @@ EXPORTS = (
     "sh_default_params", "sh_create", "sh_destroy", "sh_set_psi", "sh_set_psi_device", "sh_get_psi",
     "sh_get_psi_device", "sh_step", "sh_step_async", "sh_run", "sh_energy", "sh_energy_trace", "sh_l1",
     "sh_surface_step", "sh_local_amplitude", "sh_adjoint", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
-    "sh_l1_noalloc", "sh_profile_steps", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
+    "sh_l1_noalloc", "sh_profile_steps", "sh_residency", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
 )
 
 
@@ -84,6 +84,7 @@ def load() -> C.CDLL:
         "sh_stream": (vp, [vp]),
         "sh_steps_taken": (C.c_longlong, [vp]),
         "sh_kernel_launches": (C.c_int, [vp, C.POINTER(C.c_longlong)]),
+        "sh_residency": (C.c_int, [vp, C.POINTER(C.c_int)]),
         "sh_last_error": (C.c_char_p, [vp]),
         "sh_version": (C.c_char_p, []),
     }

@@ -496,6 +496,12 @@ void* sh_stream(sh_handle* h) { return (h && h->s) ? static_cast<void*>(h->s->st
 
 long long sh_steps_taken(sh_handle* h) { return (h && h->s) ? h->s->steps : -1; }
 
+int sh_residency(sh_handle* h, int* out) {
+  ApiRange range_("sh_residency");
+  if (!h || !h->s || !out) return fail(h, SH_EINVAL, "null argument");
+  return h->s->residency(out);
+}
+
 int sh_kernel_launches(sh_handle* h, long long* count) {
   if (!h || !h->s || !count) return SH_EINVAL;
   *count = h->s->launches;

@@ -117,6 +117,7 @@ struct SolverBase {
   virtual int surface_step(int* z, double* vn, double* hh, double* kk) = 0;
   virtual int adjoint(const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every, double* g_eps,
                       double* g_q0, double* g_psi0) = 0;
+  virtual int residency(int* out) = 0;
 };
 
 template <typename T, int N, int CL, bool DCT>
@@ -344,6 +345,41 @@ struct Solver final : SolverBase {
     cfg.numAttrs = use_pdl ? 1 : 0;
     SHB_CUDA(cudaLaunchKernelEx(&cfg, pencil_fn<MODE>(), a));
     ++launches;
+    return SH_OK;
+  }
+
+  // CTAs per SM of the step kernels and, for the clustered plane pass, the
+  // clusters the GPU holds at once (its GPCs place whole clusters only)
+  int residency(int* out) override {
+    int dev = 0, sms = 0, pb = 0, qb = 0, nc = 0;
+    SHB_CUDA(cudaGetDevice(&dev));
+    SHB_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    SHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&pb, plane_fn<kPlaneStep>(), PC::THREADS, PC::SMEM));
+    SHB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&qb, pencil_fn<kPencilStep>(), QC::THREADS,
+                                                           QC::smem(kPencilStep)));
+    if (CL > 1) {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(N * CL, p.batch, 1);
+      cfg.blockDim = dim3(PC::THREADS, 1, 1);
+      cfg.dynamicSmemBytes = PC::SMEM;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeClusterDimension;
+      attr[0].val.clusterDim.x = CL;
+      attr[0].val.clusterDim.y = 1;
+      attr[0].val.clusterDim.z = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = 1;
+      SHB_CUDA(cudaOccupancyMaxActiveClusters(&nc, plane_fn<kPlaneStep>(), &cfg));
+    } else {
+      nc = pb * sms;
+    }
+    out[0] = pb;
+    out[1] = nc;
+    out[2] = CL;
+    out[3] = N * CL * p.batch;
+    out[4] = qb;
+    out[5] = QC::TILES * p.batch;
+    out[6] = sms;
     return SH_OK;
   }
 

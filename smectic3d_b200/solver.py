@@ -144,6 +144,16 @@ class Solver:
         self._chk(self.lib.sh_profile_steps(self.h, int(nsteps), C.byref(a), C.byref(b)))
         return a.value, b.value
 
+    def residency(self) -> dict:
+        """CTAs per SM and waves of the two step kernels on this GPU."""
+        o = (C.c_int * 7)()
+        self._chk(self.lib.sh_residency(self.h, o))
+        plane_res = o[1] * o[2]
+        return {"plane_ctas_per_sm": o[0], "plane_clusters_resident": o[1], "plane_cluster": o[2],
+                "plane_ctas": o[3], "plane_waves": o[3] / plane_res if plane_res else None,
+                "pencil_ctas_per_sm": o[4], "pencil_ctas": o[5],
+                "pencil_waves": o[5] / (o[4] * o[6]) if o[4] else None, "sms": o[6]}
+
     def synchronize(self):
         self._chk(self.lib.sh_synchronize(self.h))
 
