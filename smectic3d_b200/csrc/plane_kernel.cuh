@@ -591,27 +591,24 @@ struct PlaneOps {
       }
     } else {
       fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return col_in(buf, xs, line, mk_perm<N>(i)); });
-      // the pairing goes through shared memory here: the register version
-      // spills at three CTAs per SM
-      __syncwarp();
+      // REDFT10 post-processing, one slot at a time: the partner (N - k) mod N
+      // of each slot comes from lane (G - t) mod G by a warp shuffle (lane 0
+      // holds its own partners, as in mirror_partners), and the result goes
+      // straight to the line; v is only read, so no partner array is held
+      __syncwarp();  // every lane of the line has finished reading it in the last pass
+      constexpr int NB = E / RL;
+      const int src = (G - t) & (G - 1);
 #pragma unroll
-      for (int b = 0; b < E / RL; ++b)
-#pragma unroll
-        for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
-      __syncwarp();
-#pragma unroll
-      for (int b = 0; b < E / RL; ++b)
+      for (int b = 0; b < NB; ++b)
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
           const int k = out_index<N, -1>(t, b, r);
-          cplx<T> w = tw.d[k];
-          v[b * RL + r] = cadd<T>(cmul<T>(L[pad(k)], w), cmul<T>(L[pad((N - k) & (N - 1))], conjg<T>(w)));
+          const cplx<T> q = shfl_c<T>(v[(NB - 1 - b) * RL + (RL - 1 - r)], src, G);
+          const int zs = b == 0 ? (RL - r) % RL : (NB - b) * RL + (RL - 1 - r);
+          const cplx<T> pm = t == 0 ? v[zs] : q;
+          const cplx<T> w = tw.d[k];
+          L[pad(k)] = cadd<T>(cmul<T>(v[b * RL + r], w), cmul<T>(pm, conjg<T>(w)));
         }
-      __syncwarp();
-#pragma unroll
-      for (int b = 0; b < E / RL; ++b)
-#pragma unroll
-        for (int r = 0; r < RL; ++r) L[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
       __syncthreads();
     }
     const int c0 = rank * NC;
