@@ -31,6 +31,7 @@ class _Evolve(torch.autograd.Function):
             s.step(int(nsteps))
             psiT = s.get_psi()
         ctx.p, ctx.nsteps, ctx.ckpt_every = p, int(nsteps), int(ckpt_every)
+        ctx.scalar_like = ((eps.dtype, eps.device), (q0.dtype, q0.device))
         ctx.save_for_backward(psi0)
         return torch.as_tensor(psiT, device=psi0.device)
 
@@ -40,9 +41,10 @@ class _Evolve(torch.autograd.Function):
         g = grad_psiT.detach().to("cpu", torch.float64).numpy()
         with Solver(ctx.p) as s:
             ge, gq, gp = s.adjoint(psi0.detach().to("cpu", torch.float64).numpy(), ctx.nsteps, g, ctx.ckpt_every)
-        dev = psi0.device
-        return (torch.as_tensor(gp, device=dev).to(psi0.dtype), torch.tensor(float(ge[0]), dtype=torch.float64),
-                torch.tensor(float(gq[0]), dtype=torch.float64), None, None, None)
+        (edt, edev), (qdt, qdev) = ctx.scalar_like
+        return (torch.as_tensor(gp, device=psi0.device).to(psi0.dtype),
+                torch.tensor(float(ge[0]), dtype=edt, device=edev),
+                torch.tensor(float(gq[0]), dtype=qdt, device=qdev), None, None, None)
 
 
 def sh_evolve(psi0: torch.Tensor, eps, q0, params: Params, nsteps: int, ckpt_every: int = 50) -> torch.Tensor:

@@ -42,3 +42,24 @@ def test_autograd_matches_sh_adjoint_and_finite_differences():
     h = 1e-4
     fd = (loss_at(-0.7 + h) - loss_at(-0.7 - h)) / (2 * h)
     assert abs(eps.grad.item() - fd) <= 1e-4 * abs(fd)
+
+
+def test_autograd_on_device_tensors():
+    """Inputs on cuda:0 get their gradients on cuda:0, equal to the host case."""
+    torch = pytest.importorskip("torch")
+    from smectic3d_b200.torch_adjoint import sh_evolve
+    n, steps = 16, 4
+    p = S.Params(n=n, precision="fp64", dt=0.05)
+    init = torch.tensor(S.ic.noise(n, 5, 0.2))
+    grads = []
+    for dev in ("cpu", "cuda:0"):
+        psi0 = init.clone().to(dev).requires_grad_(True)
+        eps = torch.tensor(-0.3, dtype=torch.float64, device=dev, requires_grad=True)
+        q0 = torch.tensor(1.0, dtype=torch.float64, device=dev, requires_grad=True)
+        out = sh_evolve(psi0, eps, q0, p, steps, ckpt_every=2)
+        assert out.device == psi0.device
+        (out ** 2).sum().backward()
+        assert psi0.grad.device == psi0.device and eps.grad.device == eps.device and q0.grad.device == q0.device
+        grads.append((psi0.grad.cpu().numpy(), eps.grad.item(), q0.grad.item()))
+    assert np.array_equal(grads[0][0], grads[1][0])
+    assert grads[0][1] == grads[1][1] and grads[0][2] == grads[1][2]
