@@ -365,6 +365,36 @@ struct PlaneOps {
     cplx<T> v[E];
     if constexpr (!DCT) {
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return L[pad(i)]; });
+    } else if constexpr (E / radix_of<N, +1, 0>() == 1) {
+      // REDFT01 input formed in registers: load the line into the first-pass
+      // slots (slot r holds i = t + G r), then take each partner N - i from
+      // lane (G - t) mod G, slot E-1-r, by a warp shuffle.  Lane 0 holds its
+      // own partners (slot (E - r) mod E), so it pairs slots r+1 and E-1-r in
+      // step r; its slot 0 (i = 0, no partner) is already final.  Every slot
+      // a shuffle reads is still unmodified in its lane.
+      const int src = (G - t) & (G - 1);
+#pragma unroll
+      for (int r = 0; r < E; ++r) v[r] = L[pad(t + G * r)];
+#pragma unroll
+      for (int r = 0; r < E / 2; ++r) {
+        const int B = E - 1 - r;
+        const cplx<T> qB = shfl_c<T>(v[B], src, G);
+        const cplx<T> qA = shfl_c<T>(v[r], src, G);
+        const bool z = t == 0;
+        const int iA = t + G * (r + (z ? 1 : 0)), iB = t + G * B;
+        const cplx<T> aA = z ? v[r + 1] : v[r];
+        const cplx<T> pB = z ? v[r + 1] : qA;
+        const cplx<T> aB = v[B];
+        cplx<T> wA = tw.d[iA], wB = tw.d[iB];
+        wA.y = -wA.y;
+        wB.y = -wB.y;
+        const cplx<T> oA = cmul<T>(mk<T>(aA.x + qB.y, aA.y - qB.x), wA);  // iA, iB > 0
+        const cplx<T> oB = cmul<T>(mk<T>(aB.x + pB.y, aB.y - pB.x), wB);
+        if (z) v[r + 1] = oA;
+        else v[r] = oA;
+        v[B] = oB;
+      }
+      fft_regs<T, N, +1>(v, L, t, tw.i);
     } else {
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return dct3_pre<T, N>(L, i, tw.d); });
     }
