@@ -134,7 +134,7 @@ int sh_local_amplitude(sh_handle* h, int nw, double* out);
  * dl_dpsi_t (e.g. psi^T - target for 1/2 ||psi^T - target||^2), recomputing
  * the forward states from checkpoints taken every `ckpt_every` steps.
  * Outputs per replica: dL/d eps, dL/d q0 (FP64 accumulation) and dL/d psi0
- * (batch*N^3).  No counterpart in the reference (BASELINE differentiation
+ * (batch*N^3).  No counterpart in the reference (a differentiation
  * addition); the forward pass is the reference loop (periodicFFT/pf3dVal.cpp:270-301). */
 int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every,
                double* g_eps, double* g_q0, double* g_psi0);

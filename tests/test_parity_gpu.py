@@ -114,7 +114,7 @@ def test_live_oracle_100_steps(n, boundary, prec):
 
 @pytest.mark.parametrize("prec", ["fp64", "fp32"])
 @pytest.mark.parametrize("boundary", ["periodic", "neumann"])
-def test_live_oracle_256_baseline_ics(boundary, prec):
+def test_live_oracle_256_workload_ics(boundary, prec):
     """The 256^3 workloads' own initial conditions, a few steps against the oracle."""
     n = 256
     p = S.Params(n=n, boundary=boundary, precision=prec, dt=0.05)
