@@ -1,0 +1,66 @@
+"""Host logic of the cluster-size autotuner (no GPU): the fastest built
+variant wins, variants that fail to build are skipped, results are cached per
+(GPU, shape) and reused."""
+import json
+
+import pytest
+
+import smectic3d_b200 as S
+from smectic3d_b200 import autotune
+
+
+@pytest.fixture
+def fake(monkeypatch, tmp_path):
+    cache = tmp_path / "tuned.json"
+    monkeypatch.setenv("SMECTIC_B200_CACHE", str(cache))
+    monkeypatch.setattr(autotune, "_gpu_name", lambda: "FakeGPU")
+    calls = []
+
+    def timer(us):
+        def _time_variant(p, v, steps):
+            calls.append(v)
+            if us[v] is None:
+                raise RuntimeError("variant not built")
+            return us[v] * 1e-6
+        return _time_variant
+    return cache, calls, timer
+
+
+def test_fastest_variant_wins_and_is_cached(fake, monkeypatch):
+    cache, calls, timer = fake
+    monkeypatch.setattr(autotune, "_time_variant", timer({4: 250.0, 8: 200.0, 16: 210.0}))
+    p = S.Params(n=256, boundary="neumann", precision="fp32")
+    rec = autotune.tune(p, steps=3)
+    assert rec["variant"] == 8
+    assert set(rec["us_per_step"]) == {"4", "8", "16"}
+    assert calls == [4, 8, 16]
+    stored = json.loads(cache.read_text())
+    assert list(stored) == ["FakeGPU|n=256|b=1|neumann|fp32|adv=0"]
+    # a second call reads the cache and times nothing
+    assert autotune.tune(p, steps=3) == rec and calls == [4, 8, 16]
+    assert autotune.best_variant(p) == 8
+    # use_cache=False times again
+    autotune.tune(p, steps=3, use_cache=False)
+    assert calls == [4, 8, 16, 4, 8, 16]
+
+
+def test_unbuilt_variants_are_skipped(fake, monkeypatch):
+    _, _, timer = fake
+    monkeypatch.setattr(autotune, "_time_variant", timer({1: 30.0, 2: None, 4: 25.0}))
+    rec = autotune.tune(S.Params(n=128, precision="fp64"), steps=3)
+    assert rec["variant"] == 4 and "2" not in rec["us_per_step"]
+
+
+def test_no_variant_raises(fake, monkeypatch):
+    _, _, timer = fake
+    monkeypatch.setattr(autotune, "_time_variant", timer({1: None, 2: None}))
+    with pytest.raises(RuntimeError, match="no plane-pass variant"):
+        autotune.tune(S.Params(n=64, precision="fp32"), steps=3)
+
+
+def test_keys_separate_shapes(fake, monkeypatch):
+    cache, _, timer = fake
+    monkeypatch.setattr(autotune, "_time_variant", timer({1: 10.0, 2: 5.0}))
+    autotune.tune(S.Params(n=64, precision="fp32", batch=8), steps=3)
+    autotune.tune(S.Params(n=64, precision="fp32", batch=8, boundary="neumann"), steps=3)
+    assert len(json.loads(cache.read_text())) == 2

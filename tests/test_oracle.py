@@ -289,3 +289,21 @@ def test_golden_64_regenerates_from_its_seed():
     o = O.NeumannOracle(ic.hyperboloid(n, p.dx, r0_cells=12.0, seed=12), p)
     o.run(int(d["steps"]))
     assert np.allclose(o.psi[::4, ::4, ::4], d["psi_sub"], rtol=0, atol=1e-13)
+
+
+def test_sine_transforms_through_the_cosine_pair():
+    """RODFT10^3(S) is REDFT10^3 of (-1)^(x+y+z) S read at reversed indices, and
+    RODFT01^3(X) is (-1)^(x+y+z) times REDFT01^3 of X reversed: a sine-transform
+    Stokes solve on the Neumann box needs no transform beyond the cosine pair."""
+    rng = np.random.default_rng(3)
+    n = 12
+    i = np.arange(n)
+    sign = (-1.0) ** (i[:, None, None] + i[None, :, None] + i[None, None, :])
+    s = rng.standard_normal((n, n, n))
+    a = sfft.dstn(s, type=2)
+    b = sfft.dctn(sign * s, type=2)[::-1, ::-1, ::-1]
+    assert np.abs(a - b).max() <= 1e-12 * np.abs(a).max()
+    x = rng.standard_normal((n, n, n))
+    c = sfft.dstn(x, type=3)
+    d = sign * sfft.dctn(x[::-1, ::-1, ::-1], type=3)
+    assert np.abs(c - d).max() <= 1e-12 * np.abs(c).max()
