@@ -366,8 +366,9 @@ struct PlaneOps {
     if constexpr (!DCT) {
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return L[pad(i)]; });
     } else if constexpr (E / radix_of<N, +1, 0>() == 1) {
-      // REDFT01 input formed in registers: load the line into the first-pass
-      // slots (slot r holds i = t + G r), then take each partner N - i from
+      // REDFT01 input exp(+i pi i/2N) (X[i] - i X[N-i]) (as dct3_pre) formed in
+      // registers: load the line into the first-pass slots (slot r holds
+      // i = t + G r), then take each partner N - i from
       // lane (G - t) mod G, slot E-1-r, by a warp shuffle.  Lane 0 holds its
       // own partners (slot (E - r) mod E), so it pairs slots r+1 and E-1-r in
       // step r; its slot 0 (i = 0, no partner) is already final.  Every slot
