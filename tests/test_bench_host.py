@@ -1,0 +1,50 @@
+"""Host logic of the benchmark (no GPU): the algorithmic byte model behind the
+roofline, the peak it divides by, and the workload parameters."""
+import json
+import math
+import sys
+from pathlib import Path
+
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parents[1]))
+import bench  # noqa: E402
+
+
+def test_algorithmic_bytes_neumann_and_periodic():
+    a = bench.algorithmic_bytes("neumann", 256, 1, "fp32")
+    r = 4 * 256 ** 3                       # one real field R
+    assert a == {"pencil": 4 * r, "plane": 2 * r, "field": r}
+    assert a["plane"] == 134217728         # the bench line's algorithmic_bytes_per_launch
+    p = bench.algorithmic_bytes("periodic", 128, 1, "fp64")
+    h = 2 * 8 * 128 * 128 * 65             # one half spectrum H
+    assert p["pencil"] + p["plane"] == 6 * h
+    b = bench.algorithmic_bytes("periodic", 64, 64, "fp32")
+    assert b["field"] == 64 * 2 * 4 * 64 * 64 * 33
+
+
+def test_peak_from_measured_file_or_fallback(tmp_path, monkeypatch):
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.peaks() == (6650.0, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"hbm_gbs": 6450.0}))
+    assert bench.peaks() == (6450.0, "measured")
+
+
+def test_workload_parameters():
+    p = bench.params_for("neumann256")
+    assert (p.n, p.batch, p.boundary, p.precision) == (256, 1, "neumann", "fp32")
+    assert p.dt == 0.05 and p.eps == -0.75 and p.beta == 2.0 and p.gamma == 1.0 and p.q0 == 1.0
+    assert p.dx == pytest.approx(2 * math.pi / 8)
+    assert bench.params_for("neumann256", "fp64").precision == "fp64"
+    q = bench.params_for("batch64")
+    assert q.batch == 64 and len(q.eps_per_replica) == 64
+    assert q.eps_per_replica[0] == pytest.approx(-0.9) and q.eps_per_replica[-1] == pytest.approx(-0.5)
+    assert "neumann 256^3 x1" in bench.workload_label("neumann256")
+
+
+def test_workload_ics_are_seeded():
+    import numpy as np
+    a = bench.make_ic("noise", 16, 3, 0.785, seed=2)
+    assert a.shape == (3, 16, 16, 16) and np.array_equal(a, bench.make_ic("noise", 16, 3, 0.785, seed=2))
+    h = bench.make_ic("hyperboloid", 16, 1, 0.785)
+    assert h.shape == (16, 16, 16)
