@@ -48,3 +48,46 @@ def test_workload_ics_are_seeded():
     assert a.shape == (3, 16, 16, 16) and np.array_equal(a, bench.make_ic("noise", 16, 3, 0.785, seed=2))
     h = bench.make_ic("hyperboloid", 16, 1, 0.785)
     assert h.shape == (16, 16, 16)
+
+
+class _FakeNvml:
+    """Read-only NVML stand-in: SM clock and clocks-event reasons per call."""
+    NVML_CLOCK_SM = 1
+
+    def __init__(self, clocks, reasons):
+        self.clocks, self.reasons, self.i = clocks, reasons, 0
+
+    def nvmlDeviceGetMaxClockInfo(self, h, kind):
+        return 1965
+
+    def nvmlDeviceGetClockInfo(self, h, kind):
+        return self.clocks[self.i % len(self.clocks)]
+
+    def nvmlDeviceGetCurrentClocksEventReasons(self, h):
+        v = self.reasons[self.i % len(self.reasons)]
+        self.i += 1
+        return v
+
+
+def test_clock_sampler_median_and_reasons(monkeypatch):
+    import time
+    fake = _FakeNvml([1965, 1950, 1965], [0x0, 0x4, 0x0])
+    s = bench.ClockSampler(0, period=0.002)
+    monkeypatch.setattr(s, "_handle", lambda: (fake, object()))
+    s.start()
+    s.begin()
+    time.sleep(0.05)
+    s.end()
+    rec = s.stop()
+    assert rec["sm_max_mhz"] == 1965 and rec["sm_mhz"] in (1950, 1965, 1957.5)
+    assert rec["reasons"] == ["sw_power_cap"] and rec["samples"] >= 3
+
+
+def test_clock_sampler_without_nvml_reports_nothing(monkeypatch):
+    s = bench.ClockSampler(0)
+
+    def broken():
+        raise RuntimeError("no NVML")
+    monkeypatch.setattr(s, "_handle", broken)
+    s.start()
+    assert s.stop() is None
