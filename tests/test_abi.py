@@ -118,6 +118,24 @@ def test_null_arguments(lib):
     assert lib.sh_default_params(None) == L.SH_EINVAL
 
 
+@pytest.mark.parametrize("name,args", [
+    ("sh_set_psi", (None, None, 0)), ("sh_set_psi_device", (None, None)), ("sh_get_psi", (None, None, 0)),
+    ("sh_get_psi_device", (None, None)), ("sh_step_async", (None, 1)), ("sh_run", (None, None, 1, None, 0)),
+    ("sh_energy", (None, None)), ("sh_energy_trace", (None, None, 1, None)), ("sh_l1", (None, None, None)),
+    ("sh_surface_step", (None, None, None, None, None)), ("sh_local_amplitude", (None, 4, None)),
+    ("sh_adjoint", (None, None, 1, None, 1, None, None, None)), ("sh_checkpoint_save", (None, None, None)),
+    ("sh_checkpoint_load", (None, None, 0)), ("sh_profile_steps", (None, 1, None, None)),
+    ("sh_residency", (None, None)), ("sh_synchronize", (None,)), ("sh_kernel_launches", (None, None)),
+])
+def test_every_handle_entry_point_rejects_a_null_handle(lib, name, args):
+    assert getattr(lib, name)(*args) == L.SH_EINVAL
+
+
+def test_handle_queries_on_a_null_handle(lib):
+    assert lib.sh_stream(None) is None
+    assert lib.sh_steps_taken(None) == -1
+
+
 def test_python_params_mapping():
     p = Params(n=64, boundary="neumann", precision="fp32", scheme="imex_euler", nonlinearity="quad_cubic",
                batch=3, eps_per_replica=(-0.9, -0.7, -0.5))
