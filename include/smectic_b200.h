@@ -190,8 +190,8 @@ int sh_profile_steps(sh_handle* h, int nsteps, double* ms_pencil, double* ms_pla
 int sh_residency(sh_handle* h, int* out);
 
 int sh_synchronize(sh_handle* h);
-void* sh_stream(sh_handle* h);               /* the handle's cudaStream_t */
-long long sh_steps_taken(sh_handle* h);
+void* sh_stream(sh_handle* h);               /* the handle's cudaStream_t (NULL handle: NULL) */
+long long sh_steps_taken(sh_handle* h);      /* steps since sh_set_psi, or as restored by sh_checkpoint_load (NULL handle: -1) */
 int sh_kernel_launches(sh_handle* h, long long* count);
 const char* sh_last_error(sh_handle* h);     /* NULL handle: last global error */
 const char* sh_version(void);
