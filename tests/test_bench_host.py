@@ -91,3 +91,32 @@ def test_clock_sampler_without_nvml_reports_nothing(monkeypatch):
     monkeypatch.setattr(s, "_handle", broken)
     s.start()
     assert s.stop() is None
+
+
+def _run_bench(args, env_extra):
+    import os
+    import subprocess
+    env = dict(os.environ, **env_extra)
+    root = Path(__file__).resolve().parents[1]
+    return subprocess.run([sys.executable, str(root / "bench.py"), *args], capture_output=True, text=True,
+                          env=env, timeout=300)
+
+
+def test_reference_arm_rank0_prints_one_line_other_ranks_nothing():
+    args = ["--impl", "reference", "--workload", "periodic128", "--steps", "1", "--warmup", "3"]
+    r1 = _run_bench(args, {"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"})
+    assert r1.returncode == 0 and r1.stdout.strip() == ""
+    r0 = _run_bench(args, {"RANK": "0", "WORLD_SIZE": "1", "LOCAL_RANK": "0"})
+    assert r0.returncode == 0, r0.stderr[-2000:]
+    lines = [ln for ln in r0.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["unit"] == "steps/s" and d["value"] > 0
+    assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
+    assert d["e2e"] == {"value": d["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert d["higher_is_better"] is True and d["metric"] == bench.METRIC
+
+
+def test_warmup_below_three_is_refused():
+    r = _run_bench(["--impl", "reference", "--warmup", "2"], {"RANK": "1"})
+    assert r.returncode != 0 and "--warmup must be >= 3" in r.stderr
