@@ -144,3 +144,11 @@ def test_python_params_mapping():
     assert [cp.eps_per_replica[i] for i in range(3)] == [-0.9, -0.7, -0.5]
     fn = Params.from_nw(256, 16)
     assert abs(fn.dx - 2 * 3.141592653589793 / 16) < 1e-15
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """No CPU fallback: without the built library the solver cannot be used."""
+    monkeypatch.setattr(L, "_lib", None)
+    monkeypatch.setattr(L, "LIB_PATH", tmp_path / "libsmectic_b200.so")
+    with pytest.raises(ImportError, match="is missing"):
+        L.load()
