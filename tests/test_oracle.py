@@ -307,3 +307,84 @@ def test_sine_transforms_through_the_cosine_pair():
     c = sfft.dstn(x, type=3)
     d = sign * sfft.dctn(x[::-1, ::-1, ::-1], type=3)
     assert np.abs(c - d).max() <= 1e-12 * np.abs(c).max()
+
+
+def test_neumann_oracle_against_the_reference_loop_literally():
+    """Two steps of cosFFT/mesabi/cosNoAdvMorph.cpp:216-231,421-442,483-530 with
+    REDFT10 / REDFT01 as explicit cosine sums (FFTW's definitions), against the
+    vectorised oracle."""
+    n, dx, dt, ep, beta, gamma, alpha, q0 = 6, 2 * math.pi / 8, 0.05, -0.3, 2.0, 1.0, 1.0, 1.0
+    p = O.Params(n=n, dx=dx, dt=dt, eps=ep, beta=beta, gamma=gamma, alpha=alpha, q0=q0)
+    psi0 = np.random.default_rng(9).uniform(-0.6, 0.6, size=(n, n, n))
+    kk, nn = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    fwd = 2.0 * np.cos(math.pi * (2 * nn + 1) * kk / (2 * n))                 # REDFT10[k, n]
+    inv = np.where(kk == 0, 1.0, 2.0) * np.cos(math.pi * (2 * nn + 1) * kk / (2 * n))
+    inv = inv.T                                                                # REDFT01[n, k]
+
+    def t3(m, a):
+        return np.einsum("ai,bj,ck,ijk->abc", m, m, m, a)
+
+    vq = [math.pi * i / (dx * n) for i in range(n)]
+    c1 = np.empty((n, n, n))
+    c2 = np.empty((n, n, n))
+    dtd2 = dt / 2
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                mq2 = vq[i] ** 2 + vq[j] ** 2 + vq[k] ** 2
+                op_sh = alpha * (mq2 - q0 * q0) ** 2
+                a_lin = ep - op_sh
+                c1[i, j, k] = 1.0 + dtd2 * a_lin
+                c2[i, j, k] = 1.0 - dtd2 * a_lin
+    scale = 1.0 / (8.0 * n ** 3)
+    psi = psi0.copy()
+    nq = t3(fwd, beta * psi ** 3 - gamma * psi ** 5)
+    for _ in range(2):
+        nq_past = nq
+        nq = t3(fwd, beta * psi ** 3 - gamma * psi ** 5)
+        psiq = t3(fwd, psi)
+        psiq = scale * (c1 * psiq + dtd2 * (3.0 * nq - nq_past)) / c2
+        psi = t3(inv, psiq)
+    orc = O.NeumannOracle(psi0, p)
+    orc.run(2)
+    assert np.abs(orc.psi - psi).max() <= 1e-13 * np.abs(psi).max()
+
+
+def test_periodic_oracle_against_the_reference_loop_literally():
+    """Two plain steps of periodicFFT/pf3dVal.cpp:129-299 (k-vectors pf3d.cpp:162-190,
+    tables :195-222, update :471-481) with the 3-D transform written as explicit
+    complex exponential sums over the full spectrum, against the vectorised
+    oracle (its r2c / c2r half-spectrum form)."""
+    n, dx, dt, ep, beta, gamma, alpha, q0 = 6, 2 * math.pi / 8, 0.05, -0.3, 2.0, 1.0, 1.0, 1.0
+    p = O.Params(n=n, dx=dx, dt=dt, eps=ep, beta=beta, gamma=gamma, alpha=alpha, q0=q0)
+    psi0 = np.random.default_rng(10).uniform(-0.6, 0.6, size=(n, n, n))
+    kk, nn = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    fwd = np.exp(-2j * math.pi * kk * nn / n)          # FFTW forward, unnormalised
+    bwd = np.exp(+2j * math.pi * kk * nn / n).T        # FFTW backward, unnormalised
+
+    def t3(m, a):
+        return np.einsum("ai,bj,ck,ijk->abc", m, m, m, a)
+
+    vq = [2 * math.pi * i / (dx * n) if i <= n // 2 else -(n - i) * 2 * math.pi / (dx * n) for i in range(n)]
+    c1 = np.empty((n, n, n))
+    c2 = np.empty((n, n, n))
+    dtd2 = dt / 2
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                mq2 = vq[i] ** 2 + vq[j] ** 2 + vq[k] ** 2
+                a_lin = ep - alpha * (mq2 - q0 * q0) ** 2
+                c1[i, j, k] = 1.0 + dtd2 * a_lin
+                c2[i, j, k] = 1.0 - dtd2 * a_lin
+    scale = 1.0 / n ** 3
+    psi = psi0.copy()
+    nq_past = t3(fwd, beta * psi ** 3 - gamma * psi ** 5)
+    for _ in range(2):
+        nq = t3(fwd, beta * psi ** 3 - gamma * psi ** 5)
+        psiq = t3(fwd, psi)
+        psiq = scale * (c1 * psiq + dtd2 * (3.0 * nq - nq_past)) / c2
+        psi = t3(bwd, psiq).real
+        nq_past = nq
+    orc = O.PeriodicOracle(psi0, p)
+    orc.run(2)
+    assert np.abs(orc.psi - psi).max() <= 1e-13 * np.abs(psi).max()
