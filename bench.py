@@ -230,6 +230,7 @@ def run_ours(args, rank, world, local_rank, dist):
     s32 = S.Solver(p32)
     s32.set_psi(psi0)
     s32.step(w)
+    s32.prepare()  # the replayed step graph is instantiated before the timed region
     l0 = s32.kernel_launches
     clocks = ClockSampler(local_rank)
     clocks.start()
@@ -243,6 +244,7 @@ def run_ours(args, rank, world, local_rank, dist):
     s64 = S.Solver(params_for(args.workload, other))
     s64.set_psi(psi0)
     s64.step(w)
+    s64.prepare()
     ms64 = timed_steps(s64, k, torch, dist)
     a32 = s32.get_psi()
     a64 = s64.get_psi()
@@ -346,8 +348,12 @@ def run_ours(args, rank, world, local_rank, dist):
 def adjoint_ratio(args, torch):
     """Differentiation workload: 128^3 periodic, FP32 forward, FP64 gradient
     accumulation, dt=0.05, checkpoints every 50 steps, L = 1/2 ||psi_T - target||^2
-    with target 0.5 cos(1.05 z), psi0 = 1.328 cos(z) + U(-0.1, 0.1).  Times T forward steps and sh_adjoint over the
-    same T steps (its own forward sweep, the recompute and the reverse sweep)."""
+    with target 0.5 cos(1.05 z), psi0 = 1.328 cos(z) + U(-0.1, 0.1).  Device-timed
+    (CUDA events on the solver's stream): T plain forward steps; the forward sweep
+    that keeps the checkpoints (sh_adjoint_forward, what the autograd forward runs);
+    the backward sweep (sh_adjoint_backward: recompute from the checkpoints and the
+    reverse steps).  total_over_forward = (forward sweep + backward) / plain forward,
+    the cost of forward plus backward through torch.autograd."""
     import numpy as np
     import smectic3d_b200 as S
     n, k = 128, 50
@@ -358,21 +364,34 @@ def adjoint_ratio(args, torch):
     psi0 = 1.328 * np.cos(z)[None, None, :] + S.ic.noise(n, 0)
     target = 0.5 * np.broadcast_to(np.cos(1.05 * np.arange(n) * p.dx)[None, None, :], (n, n, n))
     with S.Solver(p) as s:
+        ext = torch.cuda.ExternalStream(s.stream)
+
+        def timed(fn):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.synchronize()
+            e0.record(ext)
+            fn()
+            e1.record(ext)
+            e1.synchronize()
+            return e0.elapsed_time(e1)
+
         s.set_psi(psi0)
         s.step(5)
+        s.prepare()
         s.set_psi(psi0)
-        s.synchronize()
-        t0 = time.perf_counter()
-        s.step(t_steps)
-        t_fwd = time.perf_counter() - t0
+        t_fwd = timed(lambda: s.step_async(t_steps))
         lam = s.get_psi() - target
-        s.adjoint(psi0, t_steps, lam, ckpt_every=k)  # warm: kernels and the adjoint's buffers
-        t0 = time.perf_counter()
-        ge, gq, _ = s.adjoint(psi0, t_steps, lam, ckpt_every=k)
-        t_adj = time.perf_counter() - t0
+        s.adjoint_forward(psi0, t_steps, k)  # warm: kernels and the adjoint's buffers
+        s.adjoint_backward(lam)
+        t_fck = timed(lambda: s.adjoint_forward(psi0, t_steps, k))
+        out = {}
+        t_bwd = timed(lambda: out.update(g=s.adjoint_backward(lam)))
+        ge, gq, _ = out["g"]
     return {"workload": f"periodic {n}^3 fp32, dt=0.05, T={t_steps}, checkpoints every {k}",
-            "forward_ms_per_step": t_fwd / t_steps * 1e3, "adjoint_ms_per_step": t_adj / t_steps * 1e3,
-            "total_over_forward": t_adj / t_fwd, "backward_over_forward": (t_adj - t_fwd) / t_fwd,
+            "timing": "CUDA events on the solver stream",
+            "forward_ms_per_step": t_fwd / t_steps, "forward_with_checkpoints_ms_per_step": t_fck / t_steps,
+            "backward_ms_per_step": t_bwd / t_steps,
+            "backward_over_forward": t_bwd / t_fwd, "total_over_forward": (t_fck + t_bwd) / t_fwd,
             "grad_eps": float(ge[0]), "grad_q0": float(gq[0])}
 
 
@@ -403,6 +422,7 @@ def other_configs(torch, steps=200):
         with S.Solver(p) as s:
             s.set_psi(psi)
             s.step(10)
+            s.prepare()
             ms = timed_steps(s, steps, torch, None)
         rate = steps / (ms / 1e3)
         b = model_bytes(p.n, p.batch, p.precision, False)
@@ -479,6 +499,7 @@ def cufft_comparator(torch, steps=100):
     with S.Solver(p) as s:
         s.set_psi(S.ic.noise(n, 0))
         s.step(10)
+        s.prepare()
         ours = steps / (timed_steps(s, steps, torch, None) / 1e3)
     return {"what": "plain periodic CNAB2 step, 256^3 FP32: torch.fft (cuFFT) + torch elementwise, unfused, "
                     "against this library's fused passes",
@@ -516,23 +537,31 @@ def cpu_baseline(workload, budget_s=20.0, max_steps=None):
                       f"in {el:.1f} s" + (f", scaled by 1/{batch} domains" if batch > 1 else "")}
 
 
-def run_reference(args, rank):
+def run_reference(args, rank, budget_s=180.0):
+    """The reference arm: the oracle port (the reference itself needs FFTW-MPI
+    + MPI, absent here) on all host cores, W untimed warm-up steps, then K
+    timed steps, or as many as fit ``budget_s`` when K steps would not."""
     if rank != 0:
         return None
-    k = min(args.steps, 30)
-    w = min(args.warmup, 3)
+    w = args.warmup
     orc, batch = _oracle_solver(args.workload)
+    t0 = time.perf_counter()
     for _ in range(w):
         orc.step()
+    per_step = (time.perf_counter() - t0) / max(w, 1)
+    k = args.steps if per_step * args.steps <= budget_s else max(1, int(budget_s / per_step))
     t0 = time.perf_counter()
     for _ in range(k):
         orc.step()
     el = time.perf_counter() - t0
     v = k / el / batch
     bnd, n, _, prec, _ = WORKLOADS[args.workload]
-    cb = {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port",
-          "sample": f"{k} steps (of the requested {args.steps}) of one {n}^3 FP64 domain, oracle port on "
-                    f"SciPy pocketfft with workers={os.cpu_count()}; the reference needs FFTW-MPI + MPI, absent here"}
+    sample = (f"{k} timed steps after {w} warm-up steps of one {n}^3 FP64 domain, oracle port on SciPy pocketfft "
+              f"with workers={os.cpu_count()}")
+    if k < args.steps:
+        sample += f" ({args.steps} requested; {k} fit the {budget_s:.0f} s budget)"
+    sample += "; the reference needs FFTW-MPI + MPI, absent here"
+    cb = {"value": v, "unit": "steps/s", "cores": os.cpu_count(), "kind": "port", "sample": sample}
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": k,
             "warmup": w, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",

@@ -41,6 +41,9 @@ extern "C" {
 /* arithmetic of fields and transforms */
 #define SH_FP64 0
 #define SH_FP32 1
+/* gradient and mixed derivatives of the Neumann curvature pass */
+#define SH_CURV_DIFFERENCE 0 /* centred differences, one-sided at the walls (cosNoAdvMorphCurv.cpp:811-940) */
+#define SH_CURV_SPECTRAL 1   /* exact derivatives of the cosine series (sine series through the cosine pair) */
 /* host array layouts of psi */
 #define SH_LAYOUT_DENSE 0  /* (i*N + j)*N + k       (cosFFT/mesabi/cosNoAdvMorph.cpp:296) */
 #define SH_LAYOUT_PADDED 1 /* (i*N + j)*2(N/2+1) + k (periodicFFT/pf3d.cpp:312)         */
@@ -54,7 +57,8 @@ typedef struct sh_params {
   int n;             /* grid points per side: 16, 32, 64, 128, 256 or 512   */
   int batch;         /* independent replicas integrated together (>= 1)     */
   int boundary;      /* SH_PERIODIC / SH_NEUMANN                             */
-  int advection;     /* 1: Stokes advection (periodic only, pf3d.cpp:399-465) */
+  int advection;     /* 1: Stokes advection (periodic: pf3d.cpp:399-465; Neumann:
+                        the sine-transform velocity of cosFFT/comet/morphSurfK.cpp) */
   int nonlinearity;  /* SH_QUINTIC / SH_QUAD_CUBIC                           */
   int scheme;        /* SH_CNAB2 / SH_IMEX_EULER                             */
   int precision;     /* SH_FP64 / SH_FP32                                    */
@@ -66,6 +70,7 @@ typedef struct sh_params {
   double sub_sigma;  /* substrate penalty sigma (cosFFT/comet/cosNoAdvMorph.cpp:67-74) */
   double sub_z0;
   const double* eps_per_replica; /* NULL, or `batch` values of epsilon       */
+  int curvature;     /* Neumann curvature pass: SH_CURV_DIFFERENCE / SH_CURV_SPECTRAL */
 } sh_params;
 
 typedef struct sh_handle sh_handle;
@@ -96,12 +101,36 @@ int sh_step(sh_handle* h, int nsteps);
 /* Enqueue `nsteps` steps on the handle's stream and return immediately. */
 int sh_step_async(sh_handle* h, int nsteps);
 
+/* Build ahead of time what sh_step_async replays for runs of 16 steps or
+ * more without per-step diagnostics (energy_trace = 0, l1_interval = 0): a
+ * CUDA graph of 16 steps, instantiated once per handle.  Runs nothing and
+ * changes no state; without this call the first such sh_step builds it.  No
+ * counterpart in the reference, whose loop has no set-up beyond its FFTW plans. */
+int sh_prepare(sh_handle* h);
+
 /* One drop-in time loop with host buffers: psi0 in, nsteps steps, psi out. */
 int sh_run(sh_handle* h, const double* host_psi0, int nsteps, double* host_psi_out, int layout);
 
 /* Lyapunov energy of the current state, one value per replica
  * (energyPsi.m:225-234 with the exact spectral Laplacian, FP64 sums). */
 int sh_energy(sh_handle* h, double* out);
+/* Dominant layer wavenumber of the current state, one value per replica: |q|
+ * of the |k| shell (width 2 pi/L periodic, pi/L Neumann; shell index = the
+ * rounded length of the mode's index vector) that holds the most spectral
+ * power, the k = 0 shell excluded; the lowest shell wins a tie.  The power of
+ * each mode is |psihat|^2 of the R2C spectrum (each kz in (0, N/2) counted
+ * twice for its conjugate) or of the REDFT10 spectrum (halved on each zero
+ * index), summed per shell in FP64.  The quantity pf3dVal's sweep probes
+ * (periodicFFT/pf3dVal.cpp:214-325) for long runs. */
+int sh_dominant_wavenumber(sh_handle* h, double* out);
+/* Stokes velocity of the current state of an advected handle (advection = 1),
+ * batch*N^3 doubles per component, dense (i, j, k) order.  Periodic: the
+ * Fourier solve of periodicFFT/pf3d.cpp:399-451.  Neumann: the sine-transform
+ * solve of cosFFT/comet/morphSurfK.cpp:686-882 (S = (L psi) grad psi with
+ * difference gradients one-sided at the walls, RODFT10, the projector with the
+ * sine wavenumbers pi (m+1)/L, RODFT01), which morphSurfK computes but does
+ * not use or write. */
+int sh_velocity(sh_handle* h, double* ux, double* uy, double* uz);
 /* Energies recorded by energy_trace: out[s*batch + r] for the first
  * min(max_steps, steps taken) steps; *count receives the number of steps. */
 int sh_energy_trace(sh_handle* h, double* out, int max_steps, int* count);
@@ -139,6 +168,18 @@ int sh_local_amplitude(sh_handle* h, int nw, double* out);
 int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every,
                double* g_eps, double* g_q0, double* g_psi0);
 
+/* The two halves of sh_adjoint, for callers that want psi^T before they know
+ * the loss (an autograd forward, then its backward).  sh_adjoint_forward sets
+ * psi0, takes nsteps steps keeping a checkpoint every ckpt_every steps, and
+ * leaves the handle at psi^T (read it with sh_get_psi).  sh_adjoint_backward
+ * runs the recompute and reverse sweep from those checkpoints for the loss
+ * gradient dl_dpsi_t at psi^T; the handle must still hold the state the
+ * forward sweep ended in (any step, sh_set_psi or sh_checkpoint_load in
+ * between returns SH_ESTATE), and is left in it, so several losses can be
+ * differentiated after one forward sweep. */
+int sh_adjoint_forward(sh_handle* h, const double* psi0, int nsteps, int ckpt_every);
+int sh_adjoint_backward(sh_handle* h, const double* dl_dpsi_t, double* g_eps, double* g_q0, double* g_psi0);
+
 /* Binary checkpoint of the full state (including the AB2 history, which the
  * reference's text files drop): query size with buf == NULL. */
 int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes);
@@ -146,15 +187,15 @@ int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes);
 
 /*
  * L1 monitor of two device psi fields that allocates no device memory.
- * No counterpart in the reference: it is the monitor of sh_l1 (the
- * reference's L1 of periodicFFT/pf3d.cpp:489-509, evaluated on caller
- * buffers) for callers that must not let a library allocate. Examples: a host
- * that manages all device memory through its own pool, and real-time loops
- * that cannot take the implicit device synchronisation of cudaMalloc/cudaFree.
+ * No counterpart in the reference. It computes, per replica,
+ *   L1 = sum |psi_new - psi_old| / (dt sum |psi_new|),
+ * the relaxation monitor that sh_l1 reports, on buffers the caller owns. It
+ * is for callers that must not let a library allocate. Examples: a host that
+ * manages all device memory through its own pool, and real-time loops that
+ * cannot take the implicit device synchronisation of cudaMalloc/cudaFree.
  *
  * dev_psi_new, dev_psi_old: batch*n3 doubles each on the current device.
- * dev_out: batch doubles on the current device; receives
- * sum|new - old| / (dt sum|new|) per replica.
+ * dev_out: batch doubles on the current device; receives L1 per replica.
  * stream: a cudaStream_t; the call is stream-ordered and returns without
  * synchronising.
  *
@@ -162,8 +203,11 @@ int sh_checkpoint_load(sh_handle* h, const void* buf, size_t bytes);
  * (256 KiB, held by every GPU that loads the library until the process
  * exits). batch is therefore at most SH_L1_NOALLOC_MAX_BATCH; larger values
  * return SH_EINVAL. The first call on a device looks up that array's device
- * address (cudaGetSymbolAddress) with the device current. Make that first call
- * before any stream capture. Each call overwrites every slot it reads, so no
+ * address (cudaGetSymbolAddress) with the device current and keeps it for the
+ * rest of the process. Make that first call before any stream capture. A
+ * cudaDeviceReset discards the array with the rest of the device state, so
+ * the kept address is stale afterwards: do not call this entry point on a
+ * device after resetting it. Each call overwrites every slot it reads, so no
  * state carries over between calls. Calls that overlap on the GPU (on
  * different streams, or on several host threads) share the array and race.
  * Errors: sh_last_error(NULL).

@@ -273,6 +273,31 @@ class PeriodicOracle:
         return grads, dtpsi, curvh, dxx, dyy, dxy
 
 
+def surface_scan_vec(psi_new, grads, dtpsi, curvh, dxx, dyy, dxy, threshold: float = 0.1):
+    """``surface_scan`` written with whole-array operations, for grids where
+    the per-column loop is too slow (equal to it, tests/test_oracle.py)."""
+    n = psi_new.shape[0]
+    k = np.arange(n)[None, None, :]
+    above = psi_new > threshold
+    has1 = above.any(axis=2)
+    k1 = np.argmax(above, axis=2)
+    neg = (psi_new < 0) & (k > k1[:, :, None])
+    found = has1 & neg.any(axis=2)
+    k2 = np.argmax(neg, axis=2)
+    ii, jj = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    km = np.maximum(k2 - 1, 0)
+    back = np.abs(psi_new[ii, jj, k2]) > np.abs(psi_new[ii, jj, km])
+    idx = np.where(back, km, k2)
+    pick = lambda f: f[ii, jj, idx]
+    gv = np.sqrt(pick(grads[0]) ** 2 + pick(grads[1]) ** 2 + pick(grads[2]) ** 2)
+    z = np.where(found, k2, -1).astype(np.int64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        vn = np.where(found, pick(dtpsi) / gv, np.nan)
+        hh = np.where(found, pick(curvh) / gv, np.nan)
+        kk = np.where(found, (pick(dxx) * pick(dyy) - pick(dxy) ** 2) / (gv * gv), np.nan)
+    return z, vn, hh, kk
+
+
 def surface_scan(psi_new, grads, dtpsi, curvh, dxx, dyy, dxy, threshold: float = 0.1):
     """Column scan of surfTrack (periodicFFT/surfTrack.cpp:767-806).
 
@@ -319,16 +344,37 @@ def idct3d(a):
     return sfft.dctn(a, type=3, workers=WORKERS)
 
 
+def kvec_dst(n: int, dx: float) -> np.ndarray:
+    """Vs[m] = pi (m + 1)/(dx N), the RODFT10 wavenumbers (cosFFT/comet/morphSurfK.cpp:331-348)."""
+    return np.pi * (np.arange(n) + 1.0) / (dx * n)
+
+
+def dst3d(a):
+    """RODFT10 in every axis (FFTW's unnormalised DST-II)."""
+    return sfft.dstn(a, type=2, workers=WORKERS)
+
+
+def idst3d(a):
+    """RODFT01 in every axis (FFTW's unnormalised DST-III)."""
+    return sfft.dstn(a, type=3, workers=WORKERS)
+
+
 class NeumannOracle:
     """cosNoAdvMorph: DCT-II forward, DCT-III inverse, scale 0.125/N^3.
 
     cosFFT/mesabi/cosNoAdvMorph.cpp:112, 216-231, 423-442, 483-530.
     Substrate penalty: cosFFT/comet/cosNoAdvMorph.cpp:67-74, 591-623.
+    advect=True: the Stokes velocity of cosFFT/comet/morphSurfK.cpp (sine
+    transforms, :331-348, 390-418, 686-770, 862-882) advects psi as the
+    periodic step does, N = beta psi^3 - gamma psi^5 - u . grad psi (the term
+    morphSurfK.cpp:893-898 carries commented out); the first history N-hat
+    has no advection, as in morphSurfK.cpp:629-636.
     """
 
-    def __init__(self, psi0: np.ndarray, p: Params):
+    def __init__(self, psi0: np.ndarray, p: Params, advect: bool = False):
         self.p = p
         self.n = p.n
+        self.advect = advect
         self.scale = 0.125 / float(self.n) ** 3
         qx, qy, qz = _grids_dct(p)
         self.qx, self.qy, self.qz = qx, qy, qz
@@ -352,17 +398,42 @@ class NeumannOracle:
             out = out + pen * self.wall
         return out
 
+    def velocity(self, psiq):
+        """Stokes velocity of the Neumann box (cosFFT/comet/morphSurfK.cpp):
+        L psi = REDFT01(scale opSH psihat) (:686-696); grad psi by centred
+        differences, one-sided at the walls (:700-766); S = (L psi) grad psi
+        through RODFT10 (:763-770); u = RODFT01(CM1 (S - CM2 (Vs . S))) with the
+        sine wavenumbers Vs = pi (m+1)/L in every axis, CM1 = scale/(rho eta |Vs|^2),
+        CM2 = Vs/|Vs|^2 (:624-631, 862-882).  Returns (u, grad, L psi)."""
+        p, s = self.p, self.scale
+        psi = self.psi
+        lpsi = idct3d(s * self.op_sh * psiq)
+        grads = tuple(_fd_wall(psi, ax, p.dx) for ax in range(3))
+        vs = kvec_dst(self.n, p.dx)
+        vx, vy, vz = vs[:, None, None], vs[None, :, None], vs[None, None, :]
+        mq2 = vx * vx + vy * vy + vz * vz
+        cm1 = s / (p.rho * p.eta * mq2)
+        sq = [dst3d(lpsi * g) for g in grads]
+        dot = vx * sq[0] + vy * sq[1] + vz * sq[2]
+        u = tuple(idst3d(cm1 * (sc - vc / mq2 * dot)) for sc, vc in zip(sq, (vx, vy, vz)))
+        return u, grads, lpsi
+
     def step(self):
         p = self.p
         nq_past = self.nq
-        nq = dct3d(self._nonlin_local(self.psi))
+        nr = self._nonlin_local(self.psi)
         psiq = dct3d(self.psi)
+        grads = u = None
+        if self.advect:
+            u, grads, _ = self.velocity(psiq)
+            nr = nr - u[0] * grads[0] - u[1] * grads[1] - u[2] * grads[2]
+        nq = dct3d(nr)
         if p.scheme == "cnab2":
             psiq_new = self.scale * (self.c1 * psiq + 0.5 * p.dt * (3.0 * nq - nq_past)) / self.c2
         else:
             psiq_new = self.scale * (psiq + p.dt * nq) / (1.0 - p.dt * self.a_lin)
         psi_new = idct3d(psiq_new)
-        self.last = {"psiq": psiq, "nq": nq, "psi_old": self.psi}
+        self.last = {"psiq": psiq, "nq": nq, "psi_old": self.psi, "u": u, "grads": grads}
         self.nq = nq
         self.psi = psi_new
         self.step_count += 1
@@ -398,7 +469,32 @@ def neumann_curvature_fields(orc: "NeumannOracle"):
             "dzz": idct3d(-s * orc.qz ** 2 * psiq), "dt": idct3d(s * (orc.a_lin * psiq + nq))}
 
 
-def neumann_curvature_scan(psi, f, dx: float, threshold: float = 0.7):
+def neumann_spectral_derivatives(psi, dx: float):
+    """First and mixed derivatives of the cosine series of psi (the REDFT01
+    expansion of scale REDFT10(psi)), exactly: d/dx turns the cosine series in x
+    into the sine series RODFT01 of X[m] = -q_{m+1} A[m+1] (m < N-1; X[N-1] = 0).
+    Returns psi_x, psi_y, psi_z, psi_xy, psi_xz, psi_yz."""
+    n = psi.shape[0]
+    a = dct3d(psi) / (8.0 * n ** 3)
+    q = kvec_dct(n, dx)
+
+    def dsin(b, ax):
+        b = np.moveaxis(b, ax, 0)
+        out = np.zeros_like(b)
+        out[:-1] = -q[1:].reshape((-1,) + (1,) * (b.ndim - 1)) * b[1:]
+        return np.moveaxis(out, 0, ax)
+
+    def inv(b, sine_axes):
+        for ax in range(3):
+            b = (sfft.dst if ax in sine_axes else sfft.dct)(b, type=3, axis=ax, workers=WORKERS)
+        return b
+
+    ax_, ay_, az_ = dsin(a, 0), dsin(a, 1), dsin(a, 2)
+    return (inv(ax_, (0,)), inv(ay_, (1,)), inv(az_, (2,)), inv(dsin(ax_, 1), (0, 1)), inv(dsin(ax_, 2), (0, 2)),
+            inv(dsin(ay_, 2), (1, 2)))
+
+
+def neumann_curvature_scan(psi, f, dx: float, threshold: float = 0.7, spectral=None):
     """Column scan of the Neumann curvature pass (cosNoAdvMorphCurv.cpp:874-965).
 
     For each (i, j) scan -z from the top for the first psi < 0 after
@@ -411,10 +507,14 @@ def neumann_curvature_scan(psi, f, dx: float, threshold: float = 0.7):
     of psi can be stale there).  Where the reference's z formula would read
     past the top of the column (k2 = N-1 with k interior) the one-sided
     backward formula is used.  Returns z = k2, v_n, H, K (-1 / NaN when no
-    crossing)."""
+    crossing).  ``spectral`` (neumann_spectral_derivatives(psi, dx)) replaces
+    the difference gradient and mixed derivatives by the exact ones of the
+    cosine series."""
     n = psi.shape[0]
     gx, gy = _fd_wall(psi, 0, dx), _fd_wall(psi, 1, dx)
     gz = _fd_wall(psi, 2, dx)
+    if spectral is not None:
+        gx, gy, gz = spectral[:3]
     td = 2 * dx
     z = -np.ones((n, n), dtype=np.int64)
     vn = np.full((n, n), np.nan)
@@ -446,6 +546,8 @@ def neumann_curvature_scan(psi, f, dx: float, threshold: float = 0.7):
                     else:
                         dxz = 2 * (gx[i, j, k2] - gx[i, j, k2 - 1]) / td
                         dyz = 2 * (gy[i, j, k2] - gy[i, j, k2 - 1]) / td
+                    if spectral is not None:
+                        dxy, dxz, dyz = spectral[3][i, j, k2], spectral[4][i, j, k2], spectral[5][i, j, k2]
                     xx, yy, zz = f["dxx"][i, j, k2], f["dyy"][i, j, k2], f["dzz"][i, j, k2]
                     z[i, j] = k2
                     vn[i, j] = f["dt"][i, j, k2] / g
@@ -595,6 +697,24 @@ def dominant_wavenumber(psi, dx: float) -> float:
     w[n // 2] = 1.0
     ph = ph * w[None, None, :]
     dq = 2.0 * np.pi / (n * dx)
+    shell = np.rint(mq / dq).astype(np.int64)
+    power = np.bincount(shell.ravel(), weights=ph.ravel())
+    power[0] = 0.0
+    return float(np.argmax(power) * dq)
+
+
+def dominant_wavenumber_neumann(psi, dx: float) -> float:
+    """The same shell argmax for the Neumann box: REDFT10 spectrum, q = pi m / L,
+    shells of width pi / L, the power of each mode weighted as in Parseval's
+    sum of the REDFT10 pair (1/2 on every zero index)."""
+    n = psi.shape[0]
+    q = kvec_dct(n, dx)
+    mq = np.sqrt(q[:, None, None] ** 2 + q[None, :, None] ** 2 + q[None, None, :] ** 2)
+    x = dct3d(psi)
+    w = np.ones(n)
+    w[0] = 0.5
+    ph = x * x * (w[:, None, None] * w[None, :, None] * w[None, None, :])
+    dq = np.pi / (n * dx)
     shell = np.rint(mq / dq).astype(np.int64)
     power = np.bincount(shell.ravel(), weights=ph.ravel())
     power[0] = 0.0

@@ -17,12 +17,13 @@ SH_QUINTIC, SH_QUAD_CUBIC = 0, 1
 SH_CNAB2, SH_IMEX_EULER = 0, 1
 SH_FP64, SH_FP32 = 0, 1
 SH_LAYOUT_DENSE, SH_LAYOUT_PADDED = 0, 1
+SH_CURV_DIFFERENCE, SH_CURV_SPECTRAL = 0, 1
 
 # every entry point include/smectic_b200.h declares
 EXPORTS = (
     "sh_default_params", "sh_create", "sh_destroy", "sh_set_psi", "sh_set_psi_device", "sh_get_psi",
-    "sh_get_psi_device", "sh_step", "sh_step_async", "sh_run", "sh_energy", "sh_energy_trace", "sh_l1",
-    "sh_surface_step", "sh_local_amplitude", "sh_adjoint", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
+    "sh_get_psi_device", "sh_step", "sh_step_async", "sh_prepare", "sh_run", "sh_energy", "sh_dominant_wavenumber", "sh_velocity", "sh_energy_trace", "sh_l1",
+    "sh_surface_step", "sh_local_amplitude", "sh_adjoint", "sh_adjoint_forward", "sh_adjoint_backward", "sh_checkpoint_save", "sh_checkpoint_load", "sh_host_alloc", "sh_host_free",
     "sh_l1_noalloc", "sh_profile_steps", "sh_residency", "sh_synchronize", "sh_stream", "sh_steps_taken", "sh_kernel_launches", "sh_last_error", "sh_version",
 )
 
@@ -35,7 +36,7 @@ class ShParams(C.Structure):
         ("dx", C.c_double), ("dt", C.c_double), ("eps", C.c_double), ("beta", C.c_double),
         ("gamma", C.c_double), ("alpha", C.c_double), ("q0", C.c_double), ("eta", C.c_double),
         ("rho", C.c_double), ("w_mid", C.c_double), ("sub_sigma", C.c_double), ("sub_z0", C.c_double),
-        ("eps_per_replica", C.POINTER(C.c_double)),
+        ("eps_per_replica", C.POINTER(C.c_double)), ("curvature", C.c_int),
     ]
 
 
@@ -67,13 +68,18 @@ def load() -> C.CDLL:
         "sh_get_psi_device": (C.c_int, [vp, vp]),
         "sh_step": (C.c_int, [vp, C.c_int]),
         "sh_step_async": (C.c_int, [vp, C.c_int]),
+        "sh_prepare": (C.c_int, [vp]),
         "sh_run": (C.c_int, [vp, vp, C.c_int, vp, C.c_int]),
         "sh_energy": (C.c_int, [vp, dp]),
+        "sh_dominant_wavenumber": (C.c_int, [vp, dp]),
+        "sh_velocity": (C.c_int, [vp, vp, vp, vp]),
         "sh_energy_trace": (C.c_int, [vp, dp, C.c_int, ip]),
         "sh_l1": (C.c_int, [vp, dp, ip]),
         "sh_surface_step": (C.c_int, [vp, ip, dp, dp, dp]),
         "sh_local_amplitude": (C.c_int, [vp, C.c_int, dp]),
         "sh_adjoint": (C.c_int, [vp, vp, C.c_int, vp, C.c_int, dp, dp, vp]),
+        "sh_adjoint_forward": (C.c_int, [vp, vp, C.c_int, C.c_int]),
+        "sh_adjoint_backward": (C.c_int, [vp, vp, dp, dp, vp]),
         "sh_checkpoint_save": (C.c_int, [vp, vp, C.POINTER(C.c_size_t)]),
         "sh_checkpoint_load": (C.c_int, [vp, vp, C.c_size_t]),
         "sh_host_alloc": (C.c_int, [C.c_size_t, C.POINTER(vp)]),

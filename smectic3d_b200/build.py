@@ -23,7 +23,7 @@ INCLUDE = PKG.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O2",
-           "-DSHB_WITH_512", f"-I{INCLUDE}"]
+           f"-I{INCLUDE}"]
 
 
 def nvcc() -> str:

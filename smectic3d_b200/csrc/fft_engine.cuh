@@ -122,6 +122,22 @@ __host__ __device__ constexpr int tw_offset() {
 template <int N, int DIR>
 __host__ __device__ constexpr int tw_size() { return tw_offset<N, DIR, Plan<N>::P>(); }
 
+// A plan whose radix sequence reads the same both ways (16 = 4 x 4, 256 = 16 x 16)
+// has the same pass structure forward and inverse, so its inverse twiddles are
+// the conjugates of the forward ones: only the forward table is staged.
+template <int N>
+__host__ __device__ constexpr bool tw_shared() {
+  for (int s = 0; s < Plan<N>::P; ++s)
+    if (Plan<N>::R[s] != Plan<N>::R[Plan<N>::P - 1 - s]) return false;
+  return true;
+}
+// entries staged in shared memory: forward table, inverse table unless shared,
+// and the quarter-wave table for the cosine transforms
+template <int N>
+__host__ __device__ constexpr int tw_staged(bool dct) {
+  return tw_size<N, -1>() + (tw_shared<N>() ? 0 : tw_size<N, +1>()) + (dct ? N : 0);
+}
+
 // Twiddle tables of one transform length, staged in shared memory per CTA:
 // forward pass table, inverse pass table, quarter-wave exp(-i pi k / 2N).
 template <typename T>
@@ -162,16 +178,21 @@ void host_twiddles(Vec& out) {
   }
 }
 
-// copy the first ``count`` entries of the device table into shared memory
-// (caller syncs); the periodic transforms stop before the quarter-wave part
+// copy the tables a kernel uses (tw_staged entries) from the device table
+// [forward | inverse | quarter-wave] into shared memory (caller syncs); the
+// periodic transforms need no quarter-wave part
 template <typename T, int N>
 __device__ __forceinline__ TwTables<T> stage_twiddles(cplx<T>* smem, const cplx<T>* __restrict__ g, int tid, int nthr,
-                                                      int count = tw_total<N>()) {
-  for (int i = tid; i < count; i += nthr) smem[i] = __ldg(&g[i]);
+                                                      bool dct) {
+  constexpr int nf = tw_size<N, -1>(), ni = tw_size<N, +1>();
+  constexpr int nis = tw_shared<N>() ? 0 : ni;
+  for (int i = tid; i < nf + nis; i += nthr) smem[i] = __ldg(&g[i]);
+  if (dct)
+    for (int i = tid; i < N; i += nthr) smem[nf + nis + i] = __ldg(&g[nf + ni + i]);
   TwTables<T> t;
   t.f = smem;
-  t.i = smem + tw_size<N, -1>();
-  t.d = smem + tw_size<N, -1>() + tw_size<N, +1>();
+  t.i = smem + (tw_shared<N>() ? 0 : nf);
+  t.d = smem + nf + nis;
   return t;
 }
 
@@ -286,7 +307,11 @@ __device__ __forceinline__ void pass_compute(cplx<T> (&v)[Plan<N>::E], int t, co
       const int jm = (t + G * b) & (NS - 1);
       constexpr int OFF = tw_offset<N, DIR, S>();
 #pragma unroll
-      for (int r = 1; r < R; ++r) v[b * R + r] = cmul<T>(v[b * R + r], tw[OFF + (r - 1) * NS + jm]);
+      for (int r = 1; r < R; ++r) {
+        const cplx<T> w = tw[OFF + (r - 1) * NS + jm];
+        // a shared table holds the forward twiddles: the inverse uses their conjugates
+        v[b * R + r] = cmul<T>(v[b * R + r], (DIR > 0 && tw_shared<N>()) ? conjg<T>(w) : w);
+      }
     }
     DFT<T, R, DIR>::run(&v[b * R]);
   }
@@ -364,15 +389,23 @@ __device__ __forceinline__ void mirror_partners(const cplx<T> (&v)[Plan<N>::E], 
 // ``tw`` is the pass-major twiddle table of direction DIR (shared memory).
 // ``line`` is scratch for the intermediate passes (it may be the line that ld
 // reads: every read of the first pass happens before the first store).
+// First-pass input of a transform of direction DIR: element i through ld(i)
+// into its register slot (nothing else is touched, so a caller may order its
+// own synchronisation between the loads and the passes).
 template <typename T, int N, int DIR, class Loader>
-__device__ __forceinline__ void fft_line(cplx<T> (&v)[Plan<N>::E], cplx<T>* line, int t,
-                                         const cplx<T>* __restrict__ tw, Loader ld) {
+__device__ __forceinline__ void load_first(cplx<T> (&v)[Plan<N>::E], int t, Loader ld) {
   constexpr int E = Plan<N>::E, G = N / E;
   constexpr int R = radix_of<N, DIR, 0>();
 #pragma unroll
   for (int b = 0; b < E / R; ++b)
 #pragma unroll
     for (int r = 0; r < R; ++r) v[b * R + r] = ld(t + G * b + r * (N / R));
+}
+
+template <typename T, int N, int DIR, class Loader>
+__device__ __forceinline__ void fft_line(cplx<T> (&v)[Plan<N>::E], cplx<T>* line, int t,
+                                         const cplx<T>* __restrict__ tw, Loader ld) {
+  load_first<T, N, DIR>(v, t, ld);
   passes_from<T, N, DIR, 0>(line, v, t, tw);
 }
 

@@ -46,6 +46,8 @@ enum XMulKind : int {
   kXIqx = 0,     // i q_x (periodic)
   kXNegQx2 = 1,  // -q_x^2
   kXOpSH = 2,    // alpha (|q|^2 - q0^2)^2
+  kXSinDx = 3,   // Neumann: x derivative of the cosine series, as the reversed coefficients
+                 // -q_{N-k} X[N-k] (0 at k = 0) whose REDFT01 is (-1)^x psi_x
 };
 // line sets of shared memory a pencil mode uses (FFT scratch, stash, Stokes components)
 __host__ __device__ constexpr int pencil_sets(int mode) {
@@ -64,8 +66,17 @@ struct PencilCfg {
   static constexpr int RL = radix_of<N, -1, Plan<N>::P - 1>();
   static constexpr size_t SET_BYTES = size_t(TK) * LS * sizeof(cplx<T>);
   static constexpr size_t tw_off(int mode) { return SET_BYTES * pencil_sets(mode); }
-  static constexpr size_t red_off(int mode) { return tw_off(mode) + size_t(tw_total<N>()) * sizeof(cplx<T>); }
-  static constexpr size_t smem(int mode) { return red_off(mode) + 64 * sizeof(double); }
+  static constexpr size_t red_off(int mode) { return tw_off(mode) + size_t(tw_staged<N>(DCT)) * sizeof(cplx<T>); }
+  // |k| shells of the spectral-power histogram (shell = rint |index vector|):
+  // at most sqrt(3) N / 2 + 1 periodic, sqrt(3) (N - 1) + 1 Neumann
+  static constexpr int NSHELL = DCT ? 2 * N : N;
+  static constexpr size_t shell_off(int mode) { return red_off(mode) + 64 * sizeof(double); }
+  static constexpr size_t smem(int mode) {
+    return shell_off(mode) + (mode == kPencilEnergy ? size_t(NSHELL) * sizeof(double) : 0);
+  }
+  // per-CTA shared memory limit of sm_100 (the Stokes mode's three line sets
+  // do not fit at 512^3 in FP64)
+  static constexpr bool fits(int mode) { return smem(mode) <= size_t(227) * 1024; }
   // The step asks ptxas for a register budget that keeps SHB_STEP_WARPS warps
   // per SM resident in FP32 (three 256-thread CTAs at 256^3, twelve 64-thread
   // CTAs at 64^3) and SHB_STEP_WARPS_F64 in FP64 at N <= 128; every other
@@ -94,10 +105,12 @@ struct PencilArgs {
   const cplx<T>* s3[3]; // Stokes: partial stress components (forward y,z applied)
   cplx<T>* u3[3];       // Stokes: partial velocity components (may alias s3)
   double* red;          // per-CTA spectral energy partial [rep][grid.x]
+  double* shell;        // kFlShell: spectral power per |k| shell [rep][NSHELL] (accumulated, FP64)
   int* nonfinite;       // set to 1 when a new coefficient is NaN/Inf
   double coef;          // adjoint: c_{n-1} of the emitted mu combination (0 on the last reverse step)
   int xmul;             // kPencilXMul: XMulKind
   const T* q;           // wavenumber table (N entries)
+  const double* qd;     // the same wavenumbers in FP64
   const cplx<T>* tw;    // twiddle table [forward | inverse | quarter-wave]
   PointParams pp;
   int flags;
@@ -227,7 +240,7 @@ pencil_kernel(PencilArgs<T> a) {
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::red_off(MODE));
   const TwTables<T> tw =
-      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::tw_off(MODE)), a.tw, threadIdx.x, Cfg::THREADS);
+      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::tw_off(MODE)), a.tw, threadIdx.x, Cfg::THREADS, DCT);
   grid_dependency_wait();
 
   const int f0 = blockIdx.x * TK;
@@ -278,6 +291,17 @@ pencil_kernel(PencilArgs<T> a) {
     const T qyz0 = qy * qy + qz0 * qz0 - q02;
     const T qyz1 = qy * qy + qz1 * qz1 - q02;
     const bool cnab2 = a.pp.scheme == kCNAB2;
+    // FP64 values of the FP32 update (see below); the scalars stay kernel parameters
+    const double epsd = a.pp.eps[rep];
+    double qyz0d = 0.0, qyz1d = 0.0;
+    if constexpr (sizeof(T) == 4) {
+      const double qyd = __ldg(&a.qd[ky]), qz0d = __ldg(&a.qd[kz]);
+      qyz0d = qyd * qyd + qz0d * qz0d - a.pp.q0 * a.pp.q0;
+      if constexpr (DCT) {
+        const double qz1d = __ldg(&a.qd[kz + 1]);
+        qyz1d = qyd * qyd + qz1d * qz1d - a.pp.q0 * a.pp.q0;
+      }
+    }
     bool bad = false;
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
@@ -293,7 +317,40 @@ pencil_kernel(PencilArgs<T> a) {
         // psihat^{n+1} = (psihat + dt Nhat) / (1 - dt aLin),  W' = psihat^{n+1} (IMEX Euler)
         const T d0 = qx2 + qyz0;
         const T a0 = eps - alpha * d0 * d0;
-        if (cnab2) {
+        if constexpr (sizeof(T) == 4) {
+          // FP32 fields: the per-mode multipliers and the update in FP64 from the
+          // FP64 wavenumbers, one rounding of each stored result.  A multiplier
+          // rounded to FP32 repeats the same relative error every step, which
+          // drifts a mode's amplitude linearly with the step count.
+          const double hd = 0.5 * a.pp.dt;
+          const double qxd = __ldg(&a.qd[kx]);
+          const double e0 = qxd * qxd + qyz0d;
+          const double b0 = epsd - a.pp.alpha * e0 * e0;
+          if (cnab2) {
+            const double i0 = 1.0 / (1.0 - hd * b0), c0 = 1.0 + hd * b0;
+            pn.x = T((double(wv.x) + 3.0 * hd * double(nh.x)) * i0);
+            wv.x = T(c0 * double(pn.x) - hd * double(nh.x));
+            double i1 = i0, c1 = c0;
+            if constexpr (DCT) {
+              const double e1 = qxd * qxd + qyz1d;
+              const double b1 = epsd - a.pp.alpha * e1 * e1;
+              i1 = 1.0 / (1.0 - hd * b1);
+              c1 = 1.0 + hd * b1;
+            }
+            pn.y = T((double(wv.y) + 3.0 * hd * double(nh.y)) * i1);
+            wv.y = T(c1 * double(pn.y) - hd * double(nh.y));
+          } else {
+            const double i0 = 1.0 / (1.0 - a.pp.dt * b0);
+            pn.x = T((double(wv.x) + a.pp.dt * double(nh.x)) * i0);
+            double i1 = i0;
+            if constexpr (DCT) {
+              const double e1 = qxd * qxd + qyz1d;
+              i1 = 1.0 / (1.0 - a.pp.dt * (epsd - a.pp.alpha * e1 * e1));
+            }
+            pn.y = T((double(wv.y) + a.pp.dt * double(nh.y)) * i1);
+            wv = pn;
+          }
+        } else if (cnab2) {
           const T inv0 = rcp_rn(T(1) - h * a0), c10 = T(1) + h * a0;
           pn.x = (wv.x + h3 * nh.x) * inv0;
           wv.x = c10 * pn.x - h * nh.x;
@@ -336,7 +393,12 @@ pencil_kernel(PencilArgs<T> a) {
       }
     if (bad) *a.nonfinite = 1;
   } else if constexpr (MODE == kPencilEnergy) {
-    // gradient part of the energy of the current state from its partial P
+    // gradient part of the energy of the current state from its partial P,
+    // and (kFlShell) its spectral power per |k| shell
+    double* hist = reinterpret_cast<double*>(smem_raw + Cfg::shell_off(MODE));
+    const bool want_shell = (a.flags & kFlShell) != 0;
+    if (want_shell)
+      for (int i = threadIdx.x; i < Cfg::NSHELL; i += Cfg::THREADS) hist[i] = 0.0;
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
     Ops::forward(v, L, t, tw);
@@ -361,7 +423,29 @@ pencil_kernel(PencilArgs<T> a) {
           const double d1 = q02 - double(qx * qx + qy * qy + qz1 * qz1);
           acc.add(wxy * ((kz == 0 ? 0.5 : 1.0) * d0 * d0 * px * px + d1 * d1 * py * py));
         }
+        if (want_shell) {
+          // shell = rint |(ix, iy, iz)|: signed indices (Nyquist +N/2) on the periodic
+          // grid, where every kz in (0, N/2) also stands for its conjugate
+          if constexpr (!DCT) {
+            const int ix = kx <= N / 2 ? kx : kx - N, iy = ky <= N / 2 ? ky : ky - N;
+            const int sh = __double2int_rn(sqrt(double(ix * ix + iy * iy + kz * kz)));
+            const double wgt = (kz == 0 || kz == N / 2) ? 1.0 : 2.0;
+            atomicAdd(&hist[sh], wgt * (px * px + py * py));
+          } else {
+            const double wxy = (kx == 0 ? 0.5 : 1.0) * (ky == 0 ? 0.5 : 1.0);
+            const int r2 = kx * kx + ky * ky;
+            const int s0 = __double2int_rn(sqrt(double(r2 + kz * kz)));
+            const int s1 = __double2int_rn(sqrt(double(r2 + (kz + 1) * (kz + 1))));
+            atomicAdd(&hist[s0], wxy * (kz == 0 ? 0.5 : 1.0) * px * px);
+            atomicAdd(&hist[s1], wxy * py * py);
+          }
+        }
       }
+    if (want_shell) {
+      __syncthreads();
+      for (int i = threadIdx.x; i < Cfg::NSHELL; i += Cfg::THREADS)
+        if (hist[i] != 0.0) atomicAdd(&a.shell[size_t(rep) * Cfg::NSHELL + i], hist[i]);
+    }
   } else if constexpr (MODE == kPencilSpec || MODE == kPencilAdjInit || MODE == kPencilAdj) {
     Ops::load_tile(buf, a.src + plane_base, f0);
     cplx<T> lreg[E];
@@ -457,13 +541,32 @@ pencil_kernel(PencilArgs<T> a) {
     // (2N scale X for REDFT10 after REDFT01): multiply by m(q) / N (/ 2N)
     const T invn = T(1) / T(DCT ? 2 * N : N);
     const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha);
+    if constexpr (DCT) {
+      if (a.xmul == kXSinDx) {
+        // RODFT01(X)[x] = (-1)^x REDFT01(X reversed)[x] (the sine series of
+        // d/dx): slot kx takes -q_{N-kx} times coefficient N - kx, the mirror
+        // partner of kx; the plane pass applies (-1)^x
+        cplx<T> part[E];
+        mirror_partners<T, N, RL>(v, part, t);
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) {
+            const int kx = out_index<N, -1>(t, b, r);
+            const T w = kx == 0 ? T(0) : -__ldg(&a.q[N - kx]) * invn;
+            v[b * RL + r] = cscale<T>(part[b * RL + r], w);
+          }
+      }
+    }
 #pragma unroll
     for (int b = 0; b < E / RL; ++b)
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
         const T qx = __ldg(&a.q[out_index<N, -1>(t, b, r)]);
         const cplx<T> val = v[b * RL + r];
-        if (a.xmul == kXIqx) {
+        if (a.xmul == kXSinDx) {
+          // done above
+        } else if (a.xmul == kXIqx) {
           v[b * RL + r] = mk<T>(-qx * invn * val.y, qx * invn * val.x);
         } else if (a.xmul == kXNegQx2) {
           v[b * RL + r] = cscale<T>(val, -qx * qx * invn);
@@ -474,7 +577,63 @@ pencil_kernel(PencilArgs<T> a) {
         }
       }
   } else if constexpr (MODE == kPencilStokes) {
-    if constexpr (!DCT) {
+    if constexpr (DCT) {
+      // Neumann box: the stress came in as the cosine-transform partial of
+      // (-1)^(x+y+z) S, whose REDFT10 at index k is the RODFT10 of S at index
+      // N-1-k (cosFFT/comet/morphSurfK.cpp:390-418 uses RODFT10/01).  So the
+      // sine-wavenumber projector u = CM1 (S - CM2 (Vs . S)) of morphSurfK.cpp:
+      // 862-882, Vs(m) = pi (m+1)/L, reads Vs = pi (N-k)/L at index k; the
+      // inverse REDFT01 then yields (-1)^(x+y+z) u, unsigned by the plane pass.
+      cplx<T>* set[3] = {buf, buf + TK * LS, buf + 2 * TK * LS};
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Ops::load_tile(set[c], a.s3[c] + plane_base, f0);
+      __syncthreads();
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        cplx<T>* Lc = set[c] + line * LS;
+        Ops::forward(v, Lc, t, tw);
+        __syncwarp();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) Lc[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
+      }
+      __syncwarp();
+      const T q1 = __ldg(&a.q[1]);  // pi / L
+      const T sy = T(N - ky) * q1, sz0 = T(N - kz) * q1, sz1 = T(N - kz - 1) * q1;
+      const T ce = T(1.0 / a.pp.eta_rho);
+#pragma unroll
+      for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int kx = out_index<N, -1>(t, b, r);
+          const T sx = T(N - kx) * q1;
+          const int o = line * LS + pad(kx);
+          const cplx<T> px = set[0][o], py = set[1][o], pz = set[2][o];
+          // .x holds kz, .y holds kz + 1
+          const T m0 = sx * sx + sy * sy + sz0 * sz0, m1 = sx * sx + sy * sy + sz1 * sz1;
+          const T i0 = T(1) / m0, i1 = T(1) / m1;
+          const T c0 = scale * ce * i0, c1 = scale * ce * i1;
+          const T d0 = sx * px.x + sy * py.x + sz0 * pz.x;
+          const T d1 = sx * px.y + sy * py.y + sz1 * pz.y;
+          set[0][o] = mk<T>(c0 * (px.x - sx * i0 * d0), c1 * (px.y - sx * i1 * d1));
+          set[1][o] = mk<T>(c0 * (py.x - sy * i0 * d0), c1 * (py.y - sy * i1 * d1));
+          set[2][o] = mk<T>(c0 * (pz.x - sz0 * i0 * d0), c1 * (pz.y - sz1 * i1 * d1));
+        }
+#pragma unroll 1
+      for (int c = 0; c < 3; ++c) {
+        cplx<T>* Lc = set[c] + line * LS;
+        __syncwarp();
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) v[b * RL + r] = Lc[pad(out_index<N, -1>(t, b, r))];
+        Ops::inverse_to_line(v, Lc, t, tw);
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < 3; ++c) Ops::store_tile(set[c], a.u3[c] + plane_base, f0);
+    } else {
       // S -> u = scale CM1 (S - CM2 (q.S)),  CM1 = 1/(rho eta |q|^2), CM2 = q/|q|^2, both 0 at q = 0
       cplx<T>* set[3] = {buf, buf + TK * LS, buf + 2 * TK * LS};
 #pragma unroll
@@ -565,8 +724,10 @@ pencil_kernel(PencilArgs<T> a) {
     Ops::store_tile(buf, a.dst + plane_base, f0);
   } else if constexpr (MODE == kPencilStepAdv || MODE == kPencilInitAdv) {
     if constexpr (DCT) {
-      // v = scale psihat^{n+1}; emit the partials of v and of -q_x^2 v (the x
-      // half of the substrate's in-plane Laplacian), one inverse x transform each
+      // v = scale psihat^{n+1}; emit the partials of v and, where asked, of
+      // -q_x^2 v (the x half of the substrate's in-plane Laplacian) and of
+      // opSH v (L psi of the Stokes stress, cosFFT/comet/morphSurfK.cpp:686-696),
+      // one inverse x transform each
       cplx<T>* stash = buf + TK * LS + line * LS;
       __syncwarp();
 #pragma unroll
@@ -574,9 +735,11 @@ pencil_kernel(PencilArgs<T> a) {
 #pragma unroll
         for (int r = 0; r < RL; ++r) stash[pad(out_index<N, -1>(t, b, r))] = v[b * RL + r];
       __syncwarp();
-      cplx<T>* outs[2] = {a.dst, a.dst_x};
+      const T q02 = T(a.pp.q0 * a.pp.q0), alpha = T(a.pp.alpha);
+      cplx<T>* outs[3] = {a.dst, a.dst_x, a.dst_sh};
 #pragma unroll 1
-      for (int o = 0; o < 2; ++o) {
+      for (int o = 0; o < 3; ++o) {
+        if (!outs[o]) continue;  // uniform over the CTA
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -584,7 +747,15 @@ pencil_kernel(PencilArgs<T> a) {
             const int kx = out_index<N, -1>(t, b, r);
             const cplx<T> val = stash[pad(kx)];
             const T qx = __ldg(&a.q[kx]);
-            v[b * RL + r] = o == 0 ? val : cscale<T>(val, -qx * qx);
+            if (o == 0) {
+              v[b * RL + r] = val;
+            } else if (o == 1) {
+              v[b * RL + r] = cscale<T>(val, -qx * qx);
+            } else {  // the pair holds kz and kz + 1
+              const T d0 = qx * qx + qy * qy + qz0 * qz0 - q02;
+              const T d1 = qx * qx + qy * qy + qz1 * qz1 - q02;
+              v[b * RL + r] = mk<T>(alpha * d0 * d0 * val.x, alpha * d1 * d1 * val.y);
+            }
           }
         Ops::inverse_to_line(v, L, t, tw);
         __syncthreads();

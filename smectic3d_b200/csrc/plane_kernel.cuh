@@ -34,9 +34,12 @@ enum PlaneMode : int {
   kPlaneAdj = 5,
   kPlaneInvMulFwd = 6,  // inverse of (mult x src) -> real_out; times real_in[0]; forward -> dst
   kPlaneAdvN = 7,       // N(real_in[0]) - sum_c (inverse of src3[c]) real_in[1+c]; forward -> dst
+  kPlaneMulFwd = 8,     // real_in[0] real_in[1] (times the signs of sign_axes) forward -> dst
 };
 // spectral multiplier applied to the partial spectrum as the plane is loaded
-enum SpecMult : int { kMulNone = 0, kMulIqy = 1, kMulIqz = 2, kMulNegQy2 = 3, kMulNegQz2 = 4 };
+// kMulSinDy (Neumann): the sine series of d/dy as reversed coefficients,
+// element ky <- -q_{N-ky} X[N-ky] (0 at ky = 0); its REDFT01 is (-1)^y psi_y
+enum SpecMult : int { kMulNone = 0, kMulIqy = 1, kMulIqz = 2, kMulNegQy2 = 3, kMulNegQz2 = 4, kMulSinDy = 5 };
 
 
 template <typename T, int N, int CL, bool DCT>
@@ -63,20 +66,37 @@ struct PlaneCfg {
   static constexpr int BLK_B = ROWS * (NC + 1);
   static constexpr int BLK = ((BLK_A > BLK_B ? BLK_A : BLK_B) + 1) / 2 * 2;  // even: 16-byte blocks
   static constexpr size_t LB_BYTES = align_up(size_t(LINES) * LS * sizeof(cplx<T>), 128);
-  static constexpr size_t XB_BYTES = CL > 1 ? align_up(size_t(CL) * BLK * sizeof(cplx<T>), 128) : 0;
-  // With a cluster the line buffer and the send blocks share memory: the
-  // transform scratch of a phase is never live while the send blocks of the
-  // neighbouring exchange are (a barrier, and a wait for the outgoing copies,
-  // separates them).
-  static constexpr bool ALIAS = CL > 1;
-  static constexpr size_t SB_OFF = ALIAS ? 0 : LB_BYTES;
-  static constexpr size_t RB_OFF = ALIAS ? (LB_BYTES > XB_BYTES ? LB_BYTES : XB_BYTES) : SB_OFF + XB_BYTES;
-  static constexpr size_t TW_OFF = RB_OFF + XB_BYTES;
+  static constexpr size_t XB_RAW = CL > 1 ? align_up(size_t(CL) * BLK * sizeof(cplx<T>), 128) : 0;
   // the periodic transforms need no quarter-wave table
-  static constexpr int TW_ENTRIES = tw_total<N>() - (DCT ? 0 : N);
+  static constexpr int TW_ENTRIES = tw_staged<N>(DCT);
+  // block_sum scratch: one double per warp (at most 16 warps)
+  static constexpr int RED_DOUBLES = 16;
+  static constexpr size_t TAIL = size_t(TW_ENTRIES) * sizeof(cplx<T>) + 16 + 16 + RED_DOUBLES * sizeof(double);
+  // Two exchange variants between the CTAs of a cluster:
+  //  - bulk: padded send / receive blocks moved by cp.async.bulk (the default);
+  //  - direct: every thread stores its values with st.shared::cluster straight
+  //    into the line buffer of the CTA that owns them, between two cluster
+  //    barriers.  No send or receive blocks, so it fits where the bulk blocks
+  //    do not (FP64 at 512^3: a CTA owns 16 lines of 512 complex doubles).
+  static constexpr bool DIRECT = CL > 1 && 2 * (LB_BYTES > XB_RAW ? LB_BYTES : XB_RAW) + TAIL > size_t(227) * 1024;
+  // cluster size seen by the bulk-exchange machinery (none in the direct variant)
+  static constexpr int XCL = DIRECT ? 1 : CL;
+  static constexpr size_t XB_BYTES = DIRECT ? 0 : XB_RAW;
+  // With bulk exchanges shared memory holds two regions of max(line buffer,
+  // exchange blocks) each: the column-phase line buffer, which the send blocks
+  // overlay once the column transforms are done, and the receive blocks, which
+  // the scratch lines of the row phase and of the forward column phase overlay
+  // once their first pass has read them.  So the send blocks are rewritten only
+  // after a whole row phase, and a CTA never waits right after an exchange for
+  // its peers to have received its blocks.
+  static constexpr bool ALIAS = CL > 1 && !DIRECT;
+  static constexpr size_t REGION = LB_BYTES > XB_BYTES ? LB_BYTES : XB_BYTES;
+  static constexpr size_t SB_OFF = ALIAS ? 0 : LB_BYTES;
+  static constexpr size_t RB_OFF = ALIAS ? REGION : SB_OFF + XB_BYTES;
+  static constexpr size_t TW_OFF = RB_OFF + (ALIAS ? REGION : XB_BYTES);
   static constexpr size_t MB_OFF = align_up(TW_OFF + size_t(TW_ENTRIES) * sizeof(cplx<T>), 16);
   static constexpr size_t RED_OFF = MB_OFF + 16;
-  static constexpr size_t SMEM = RED_OFF + 64 * sizeof(double);
+  static constexpr size_t SMEM = RED_OFF + RED_DOUBLES * sizeof(double);
   static constexpr bool fits = SMEM <= 227 * 1024;  // per-CTA shared memory limit of sm_100
   // FP32: ptxas is asked for a register budget that keeps SHB_STEP_WARPS warps
   // per SM resident, where that many CTAs also fit the 228 KB of shared memory
@@ -128,13 +148,20 @@ struct PlaneArgs {
   int kwall;
   // kPlaneAdvN: the three velocity partials
   const cplx<T>* src3[3];
+  // Sine transforms on the Neumann box run through the cosine pair with
+  // real-space factors (-1)^x, (-1)^y, (-1)^z: on the products kPlaneMulFwd
+  // transforms, on the fields kPlaneInvReal and kPlaneAdvN invert.  Bit 0, 1, 2
+  // of sign_axes selects x, y, z (the Stokes solve of cosFFT/comet/morphSurfK.cpp
+  // uses all three; a spectral derivative the axes it differentiates).
+  int sign_axes;
+  // kPlaneInvReal, Neumann: the z transform inverts the sine series of d/dz
+  // (reversed coefficients -q_{N-k} X[N-k], 0 at k = 0)
+  int sin_dz;
   int drop_exchange;  // test hook (see Xchg::drop)
 };
 
-// Split cluster barrier.  A CTA arrives as soon as it no longer reads its
-// receive blocks (and, at the start, once its mbarriers are initialised); it
-// waits only right before copying into its peers' receive blocks.  The work
-// between the two hides the skew between the CTAs of a cluster.
+// Cluster barrier halves.  barrier.cluster arrive and wait alternate in every
+// thread; Xchg below tracks whether an arrive is outstanding.
 template <int CL>
 __device__ __forceinline__ void cluster_arrive() {
   if constexpr (CL > 1) asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
@@ -153,8 +180,60 @@ __device__ __forceinline__ uint32_t dsmem_map(const void* p, int rank) {
   return r;
 }
 
+// Store into the copy of this CTA's shared memory that belongs to cluster rank
+// ``rank`` (the direct exchange variant); a plain store without a cluster.
+template <int CL>
+__device__ __forceinline__ void st_rank(float* p, float v, int rank) {
+  if constexpr (CL == 1) { *p = v; } else {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(dsmem_map(p, rank)), "f"(v) : "memory");
+  }
+}
+template <int CL>
+__device__ __forceinline__ void st_rank(double* p, double v, int rank) {
+  if constexpr (CL == 1) { *p = v; } else {
+    asm volatile("st.shared::cluster.f64 [%0], %1;" ::"r"(dsmem_map(p, rank)), "d"(v) : "memory");
+  }
+}
+template <int CL>
+__device__ __forceinline__ void st_rank(float2* p, float2 v, int rank) {
+  if constexpr (CL == 1) { *p = v; } else {
+    asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(dsmem_map(p, rank)), "f"(v.x), "f"(v.y) : "memory");
+  }
+}
+template <int CL>
+__device__ __forceinline__ void st_rank(double2* p, double2 v, int rank) {
+  if constexpr (CL == 1) { *p = v; } else {
+    asm volatile("st.shared::cluster.v2.f64 [%0], {%1, %2};" ::"r"(dsmem_map(p, rank)), "d"(v.x), "d"(v.y) : "memory");
+  }
+}
+// Barrier around an in-place transpose of the line buffers: the CTA alone, or
+// (direct exchange) the whole cluster, whose release / acquire also orders the
+// remote stores before the reads that follow.
+template <int CL>
+__device__ __forceinline__ void transpose_sync() {
+  if constexpr (CL == 1) {
+    __syncthreads();
+  } else {
+    cluster_arrive<CL>();
+    cluster_wait<CL>();
+  }
+}
+
 // Cluster exchange state: send / receive block arrays, two mbarriers (one per
 // exchange direction) and their phase parities.
+//
+// Protocol.  The exchange copies (cp.async.bulk shared::cta -> shared::cluster)
+// complete only on the receiver's mbarrier, so a sender learns that its copies
+// have finished reading its send blocks only from the receivers.  Every CTA
+// arrives at the cluster barrier as soon as its own incoming blocks have landed
+// (end of bulk_exchange).  It waits for that phase (settle) only where it
+// rewrites its send blocks or the column line buffer they overlay, and before it
+// exits; both come after a whole row or column phase, by which time its peers
+// have long received.  When a CTA is done with its receive blocks, as data and
+// as scratch, and another exchange into them follows, it settles and arrives
+// again (xchg_rb_done); the next exchange settles that phase before it copies
+// into the peers.  The first exchange settles the arrive that publishes the
+// initialised mbarriers.  Arrive and wait strictly alternate in every thread.
 template <typename T>
 struct Xchg {
   cplx<T>* sb;
@@ -162,19 +241,48 @@ struct Xchg {
   uint64_t* mbar;
   uint32_t phases;
   int* timeout;
-  int drop;  // test hook: rank 0 sends nothing in exchange 0, so its peers' bounded waits run out
+  int drop;    // test hook: rank 0 sends nothing in exchange 0, so its peers' bounded waits run out
+  bool armed;  // an arrive is outstanding (the next cluster_wait completes it)
 };
+
+template <typename T, int CL>
+__device__ __forceinline__ void xchg_arrive(Xchg<T>& x) {
+  if constexpr (CL > 1) {
+    cluster_arrive<CL>();
+    x.armed = true;
+  }
+}
+// wait for the outstanding arrive phase, if any
+template <typename T, int CL>
+__device__ __forceinline__ void xchg_settle(Xchg<T>& x) {
+  if constexpr (CL > 1) {
+    if (x.armed) {
+      cluster_wait<CL>();
+      x.armed = false;
+    }
+  }
+}
+
+// This CTA is done with its receive blocks (another exchange into them
+// follows): wait for the outstanding phase, then arrive
+template <typename T, int CL>
+__device__ __forceinline__ void xchg_rb_done(Xchg<T>& x) {
+  if constexpr (CL > 1) {
+    xchg_settle<T, CL>(x);
+    xchg_arrive<T, CL>(x);
+  }
+}
 
 // Every thread has written its share of the send blocks; copy block d to CTA d
 // (cp.async.bulk shared::cta -> shared::cluster, completing on the receiver's
-// mbarrier ``which``) and wait until all CL incoming blocks have landed.  The
-// caller has arrived at the cluster barrier since it last read its receive
-// blocks (cluster_arrive).
+// mbarrier ``which``), wait until all CL incoming blocks have landed, and
+// arrive (the senders may reuse their send blocks once every CTA has).  The
+// settle before the copies waits for the peers' "receive blocks free" arrive.
 template <typename T, int CL>
 __device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, int blk) {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-  __syncthreads();     // every thread's send-block writes precede the copies
-  cluster_wait<CL>();  // every peer has arrived: its receive blocks are free, its mbarriers initialised
+  __syncthreads();         // every thread's send-block writes precede the copies
+  xchg_settle<T, CL>(x);   // every peer has arrived: its receive blocks are free, its mbarriers initialised
   // thread d copies block d (a copy may complete on a peer's mbarrier before
   // that peer's expect_tx: the phase completes only once both have happened)
   if (threadIdx.x < CL) {
@@ -194,18 +302,10 @@ __device__ __forceinline__ void bulk_exchange(Xchg<T>& x, int which, int rank, i
           "r"(src), "r"(bytes), "r"(rmb)
           : "memory");
     }
-    asm volatile("cp.async.bulk.commit_group;" ::: "memory");
   }
   mbar_wait_bounded(&x.mbar[which], (x.phases >> which) & 1u, x.timeout);
   x.phases ^= 1u << which;
-}
-
-// The send blocks may be rewritten once this CTA's outgoing copies read them
-// (each of the first CL threads waits for the copy it issued).
-template <int CL>
-__device__ __forceinline__ void send_blocks_free() {
-  if (threadIdx.x < CL) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-  __syncthreads();
+  xchg_arrive<T, CL>(x);  // this CTA's incoming blocks have landed
 }
 
 // z (or y) position of FFT index n in the Makhoul even/odd permutation
@@ -224,6 +324,13 @@ __device__ __forceinline__ cplx<T> dct3_pre(const cplx<T>* L, int i, const cplx<
   cplx<T> w = dtw[i];
   w.y = -w.y;
   return cmul<T>(u, w);
+}
+
+// (-1)^(x [bit 0] + y [bit 1] + z [bit 2]) of the axes in ``mask``
+template <typename T>
+__device__ __forceinline__ T axis_sign(int mask, int x, int y, int z) {
+  const int e = ((mask & 1) ? x : 0) + ((mask & 2) ? y : 0) + ((mask & 4) ? z : 0);
+  return (e & 1) ? T(-1) : T(1);
 }
 
 template <typename T, int N, int CL, bool DCT>
@@ -252,6 +359,9 @@ struct PlaneOps {
       const T qq = __ldg(&q[ky]);
       return cscale<T>(v, -qq * qq);
     }
+    if (mult == kMulSinDy) {  // v was loaded from row N - ky (col_load)
+      return ky == 0 ? mk<T>(T(0), T(0)) : cscale<T>(v, -__ldg(&q[N - ky]));
+    }
     return v;
   }
 
@@ -266,7 +376,8 @@ struct PlaneOps {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int idx = threadIdx.x + THREADS * e;
-      tmp[e] = plane[(idx / NC) * (N / 2) + c0 + idx % NC];
+      const int row = mult == kMulSinDy ? (N - idx / NC) & (N - 1) : idx / NC;  // reversed rows for d/dy
+      tmp[e] = plane[row * (N / 2) + c0 + idx % NC];
     }
     if (mult != kMulNone) {
 #pragma unroll
@@ -343,17 +454,17 @@ struct PlaneOps {
   // ---- spectral-slot access of the row and column phases ----------------
   // periodic row phase: slot k of half h (row 2q + h) of row-pair line q
   static __device__ __forceinline__ const cplx<T>& row_slot(const cplx<T>* lb, const Xchg<T>& x, int q, int h, int k) {
-    if constexpr (CL == 1) return lb[q * LS + pad(h * (N / 2) + k)];
+    if constexpr (CL == 1 || Cfg::DIRECT) return lb[q * LS + pad(h * (N / 2) + k)];
     else return x.rb[(k / NC) * Cfg::BLK + (2 * q + h) * Cfg::SA + (k % NC)];
   }
   // Neumann row phase: slot kz of row-pair line q
   static __device__ __forceinline__ const cplx<T>& row_pair(const cplx<T>* lb, const Xchg<T>& x, int q, int kz) {
-    if constexpr (CL == 1) return lb[q * LS + pad(kz)];
+    if constexpr (CL == 1 || Cfg::DIRECT) return lb[q * LS + pad(kz)];
     else return x.rb[(kz / (2 * NC)) * Cfg::BLK + q * Cfg::SA + (kz % (2 * NC))];
   }
   // forward column phase: element ky of column line c
   static __device__ __forceinline__ const cplx<T>& col_in(const cplx<T>* lb, const Xchg<T>& x, int c, int ky) {
-    if constexpr (CL == 1) return lb[c * LS + pad(ky)];
+    if constexpr (CL == 1 || Cfg::DIRECT) return lb[c * LS + pad(ky)];
     else return x.rb[(ky / ROWS) * Cfg::BLK + (ky % ROWS) * Cfg::SBs + c];
   }
 
@@ -400,9 +511,11 @@ struct PlaneOps {
       fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) { return dct3_pre<T, N>(L, i, tw.d); });
     }
     constexpr int RL = Cfg::RL_INV;
-    if constexpr (CL == 1) {
-      __syncthreads();
-      const int kc = line;
+    if constexpr (CL == 1 || Cfg::DIRECT) {
+      // in place: row y of global column kc goes to the line buffer of the CTA
+      // that owns row y (this one without a cluster), row-pair line (y mod ROWS)/2
+      transpose_sync<CL>();
+      const int kc = rank * NC + line;
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -410,16 +523,18 @@ struct PlaneOps {
           const int n = out_index<N, +1>(t, b, r);
           const cplx<T> val = v[b * RL + r];
           if constexpr (!DCT) {
-            buf[(n >> 1) * LS + pad((n & 1) * (N / 2) + kc)] = val;
+            const int yl = n % ROWS;
+            st_rank<CL>(&buf[(yl >> 1) * LS + pad((yl & 1) * (N / 2) + kc)], val, n / ROWS);
           } else {
             const int y = mk_perm<N>(n);
+            const int yl = y % ROWS;
             T* rb = reinterpret_cast<T*>(buf);
-            const int base = (y >> 1) * LS;
-            rb[2 * (base + pad(2 * kc)) + (y & 1)] = val.x;
-            rb[2 * (base + pad(2 * kc + 1)) + (y & 1)] = val.y;
+            const int base = (yl >> 1) * LS;
+            st_rank<CL>(&rb[2 * (base + pad(2 * kc)) + (yl & 1)], val.x, y / ROWS);
+            st_rank<CL>(&rb[2 * (base + pad(2 * kc + 1)) + (yl & 1)], val.y, y / ROWS);
           }
         }
-      __syncthreads();
+      transpose_sync<CL>();
     } else {
       if constexpr (Cfg::ALIAS) __syncthreads();  // every line has left the scratch the send blocks overlay
 #pragma unroll
@@ -439,18 +554,20 @@ struct PlaneOps {
             sb[2 + (yl & 1)] = val.y;
           }
         }
-      bulk_exchange<T, CL>(xs, 0, rank, Cfg::BLK);
+      bulk_exchange<T, Cfg::XCL>(xs, 0, rank, Cfg::BLK);
     }
   }
 
   // ---- row phase -------------------------------------------------------
   // inverse z transform of row pair ``line``; v slot holds psi(y0, z), psi(y0+1, z)
-  static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], const cplx<T>* buf, const Xchg<T>& xs,
-                                                     cplx<T>* L, int q, int t, const TwTables<T>& tw) {
-    if constexpr (Cfg::ALIAS) send_blocks_free<CL>();  // the scratch L overlays the outgoing send blocks
+  static __device__ __forceinline__ void row_inverse(cplx<T> (&v)[E], const cplx<T>* buf, Xchg<T>& xs,
+                                                     cplx<T>* L, int q, int t, const TwTables<T>& tw,
+                                                     const T* qt = nullptr, bool sin_dz = false) {
+    // the first pass reads the row pair into registers; the passes after it use
+    // the scratch L (for bulk exchanges a line of the receive-block region)
     if constexpr (!DCT) {
       // Z = X_a + i X_b with Hermitian extension; slot 0 holds (X[0], X[N/2])
-      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
+      load_first<T, N, +1>(v, t, [&](int i) {
         if (i == 0 || i == N / 2) {
           const cplx<T> a = row_slot(buf, xs, q, 0, 0), b = row_slot(buf, xs, q, 1, 0);
           return i == 0 ? mk<T>(a.x, b.x) : mk<T>(a.y, b.y);
@@ -460,12 +577,18 @@ struct PlaneOps {
         return i < N / 2 ? mk<T>(a.x - b.y, a.y + b.x) : mk<T>(a.x + b.y, b.x - a.y);
       });
     } else {
-      // REDFT01 input: exp(+i pi i/2N) (X[i] - i X[N-i]), X[N] = 0
-      fft_line<T, N, +1>(v, L, t, tw.i, [&](int i) {
-        const cplx<T> a = row_pair(buf, xs, q, i);
+      // REDFT01 input: exp(+i pi i/2N) (X[i] - i X[N-i]), X[N] = 0; for the
+      // sine series of d/dz X[k] is -q_{N-k} times coefficient N - k (0 at k = 0)
+      auto X = [&](int k) -> cplx<T> {
+        if (!sin_dz) return row_pair(buf, xs, q, k);
+        if (k == 0) return mk<T>(T(0), T(0));
+        return cscale<T>(row_pair(buf, xs, q, N - k), -__ldg(&qt[N - k]));
+      };
+      load_first<T, N, +1>(v, t, [&](int i) {
+        const cplx<T> a = X(i);
         cplx<T> u = a;
         if (i != 0) {
-          const cplx<T> b = row_pair(buf, xs, q, N - i);
+          const cplx<T> b = X(N - i);
           u = mk<T>(a.x + b.y, a.y - b.x);
         }
         cplx<T> w = tw.d[i];
@@ -473,6 +596,10 @@ struct PlaneOps {
         return cmul<T>(u, w);
       });
     }
+    // bulk exchanges: the scratch L overlays the receive blocks, which every
+    // line's first pass has read once the CTA has synchronised
+    if constexpr (Cfg::ALIAS) __syncthreads();
+    fft_regs<T, N, +1>(v, L, t, tw.i);
   }
 
   // z coordinate of register slot (b, r) after row_inverse (== the input slot of
@@ -511,21 +638,23 @@ struct PlaneOps {
             ob[s] = mk<T>(T(0.5) * (zk.y + zm.y), T(0.5) * (zm.x - zk.x));
           }
         }
-      if constexpr (CL == 1) {
-        __syncthreads();
-        const int y0 = 2 * line;
+      if constexpr (CL == 1 || Cfg::DIRECT) {
+        // in place: column k goes to the line buffer of the CTA that owns it
+        transpose_sync<CL>();
+        const int y0 = rank * ROWS + 2 * line;
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
           for (int r = 0; r < RL / 2; ++r) {
             const int k = out_index<N, -1>(t, b, r);
             const int s = b * (RL / 2) + r;
-            buf[k * LS + pad(y0)] = oa[s];
-            buf[k * LS + pad(y0 + 1)] = ob[s];
+            cplx<T>* col = buf + (k % NC) * LS;
+            st_rank<CL>(&col[pad(y0)], oa[s], k / NC);
+            st_rank<CL>(&col[pad(y0 + 1)], ob[s], k / NC);
           }
-        __syncthreads();
+        transpose_sync<CL>();
       } else {
-        send_blocks_free<CL>();
+        xchg_rb_done<T, Cfg::XCL>(xs);  // the row scratch overlays the receive blocks
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -536,7 +665,7 @@ struct PlaneOps {
             blk[(2 * line) * Cfg::SBs] = oa[s];
             blk[(2 * line + 1) * Cfg::SBs] = ob[s];
           }
-        bulk_exchange<T, CL>(xs, 1, rank, Cfg::BLK);
+        bulk_exchange<T, Cfg::XCL>(xs, 1, rank, Cfg::BLK);
       }
     } else {
       cplx<T>(&o)[E] = v;  // REDFT10 output, in place
@@ -550,21 +679,22 @@ struct PlaneOps {
           cplx<T> bm = cmul<T>(part[b * RL + r], conjg<T>(w));
           o[b * RL + r] = cadd<T>(a, bm);
         }
-      if constexpr (CL == 1) {
-        __syncthreads();
-        const int y0 = 2 * line;
+      if constexpr (CL == 1 || Cfg::DIRECT) {
+        transpose_sync<CL>();
+        const int y0 = rank * ROWS + 2 * line;
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
           for (int r = 0; r < RL; ++r) {
             const int k = out_index<N, -1>(t, b, r);
-            T* cb = reinterpret_cast<T*>(buf + (k >> 1) * LS);
-            cb[2 * pad(y0) + (k & 1)] = o[b * RL + r].x;
-            cb[2 * pad(y0 + 1) + (k & 1)] = o[b * RL + r].y;
+            const int pk = k >> 1;
+            T* cb = reinterpret_cast<T*>(buf + (pk % NC) * LS);
+            st_rank<CL>(&cb[2 * pad(y0) + (k & 1)], o[b * RL + r].x, pk / NC);
+            st_rank<CL>(&cb[2 * pad(y0 + 1) + (k & 1)], o[b * RL + r].y, pk / NC);
           }
-        __syncthreads();
+        transpose_sync<CL>();
       } else {
-        send_blocks_free<CL>();
+        xchg_rb_done<T, Cfg::XCL>(xs);  // the row scratch overlays the receive blocks
 #pragma unroll
         for (int b = 0; b < E / RL; ++b)
 #pragma unroll
@@ -575,21 +705,26 @@ struct PlaneOps {
             blk[2 * (2 * line) * Cfg::SBs + (k & 1)] = o[b * RL + r].x;
             blk[2 * (2 * line + 1) * Cfg::SBs + (k & 1)] = o[b * RL + r].y;
           }
-        bulk_exchange<T, CL>(xs, 1, rank, Cfg::BLK);
+        bulk_exchange<T, Cfg::XCL>(xs, 1, rank, Cfg::BLK);
       }
     }
   }
 
   // ---- column phase, forward direction ---------------------------------
-  static __device__ void col_forward_store(cplx<T>* buf, const Xchg<T>& xs, cplx<T>* __restrict__ plane, int rank,
+  static __device__ void col_forward_store(cplx<T>* buf, Xchg<T>& xs, cplx<T>* __restrict__ plane, int rank,
                                            const TwTables<T>& tw) {
-    if constexpr (Cfg::ALIAS) send_blocks_free<CL>();  // the scratch L overlays the outgoing send blocks
     const int line = threadIdx.x / G, t = threadIdx.x % G;
-    cplx<T>* L = buf + line * LS;
+    // bulk exchanges: the column lines are built in the receive-block region once
+    // every first pass has read it; the send blocks (still being read by the
+    // peers' copies) stay untouched
+    cplx<T>* cb = Cfg::ALIAS ? xs.rb : buf;
+    cplx<T>* L = cb + line * LS;
     cplx<T> v[E];
     constexpr int RL = Cfg::RL_FWD;
     if constexpr (!DCT) {
-      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return col_in(buf, xs, line, i); });
+      load_first<T, N, -1>(v, t, [&](int i) { return col_in(buf, xs, line, i); });
+      if constexpr (Cfg::ALIAS) __syncthreads();
+      fft_regs<T, N, -1>(v, L, t, tw.f);
       __syncwarp();
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
@@ -604,7 +739,7 @@ struct PlaneOps {
         for (int m = 0; m < KPT; ++m) {
           const int ky = threadIdx.x + m * THREADS;
           if (ky < N) {
-            cplx<T> z = buf[pad(ky)], zm = buf[pad((N - ky) & (N - 1))];
+            cplx<T> z = cb[pad(ky)], zm = cb[pad((N - ky) & (N - 1))];
             f0[m] = mk<T>(T(0.5) * (z.x + zm.x), T(0.5) * (z.y - zm.y));
             fn[m] = mk<T>(T(0.5) * (z.y + zm.y), T(0.5) * (zm.x - z.x));
           }
@@ -614,14 +749,16 @@ struct PlaneOps {
         for (int m = 0; m < KPT; ++m) {
           const int ky = threadIdx.x + m * THREADS;
           if (ky < N) {
-            buf[pad(ky)] = f0[m];
-            buf[NC * LS + pad(ky)] = fn[m];
+            cb[pad(ky)] = f0[m];
+            cb[NC * LS + pad(ky)] = fn[m];
           }
         }
         __syncthreads();
       }
     } else {
-      fft_line<T, N, -1>(v, L, t, tw.f, [&](int i) { return col_in(buf, xs, line, mk_perm<N>(i)); });
+      load_first<T, N, -1>(v, t, [&](int i) { return col_in(buf, xs, line, mk_perm<N>(i)); });
+      if constexpr (Cfg::ALIAS) __syncthreads();
+      fft_regs<T, N, -1>(v, L, t, tw.f);
       // REDFT10 post-processing, one slot at a time: the partner (N - k) mod N
       // of each slot comes from lane (G - t) mod G by a warp shuffle (lane 0
       // holds its own partners, as in mirror_partners), and the result goes
@@ -646,11 +783,11 @@ struct PlaneOps {
 #pragma unroll
     for (int e = 0; e < E; ++e) {
       const int idx = threadIdx.x + THREADS * e;
-      plane[(idx / NC) * (N / 2) + c0 + idx % NC] = buf[(idx % NC) * LS + pad(idx / NC)];
+      plane[(idx / NC) * (N / 2) + c0 + idx % NC] = cb[(idx % NC) * LS + pad(idx / NC)];
     }
     if constexpr (!DCT) {
       if (rank == 0) {
-        for (int ky = threadIdx.x; ky < N; ky += THREADS) plane[N * (N / 2) + ky] = buf[NC * LS + pad(ky)];
+        for (int ky = threadIdx.x; ky < N; ky += THREADS) plane[N * (N / 2) + ky] = cb[NC * LS + pad(ky)];
       }
     }
   }
@@ -707,32 +844,40 @@ plane_kernel(PlaneArgs<T> a) {
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::RED_OFF);
   const TwTables<T> tw =
-      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS,
-                           Cfg::TW_ENTRIES);
+      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS, DCT);
 
   int rank = 0;
   if constexpr (CL > 1) rank = int(cg::this_cluster().block_rank());
   Xchg<T> xs{};
-  if constexpr (CL > 1) {
+  if constexpr (CL > 1 && !Cfg::DIRECT) {
     xs.sb = reinterpret_cast<cplx<T>*>(smem_raw + Cfg::SB_OFF);
     xs.rb = reinterpret_cast<cplx<T>*>(smem_raw + Cfg::RB_OFF);
     xs.mbar = reinterpret_cast<uint64_t*>(smem_raw + Cfg::MB_OFF);
     xs.phases = 0;
     xs.timeout = a.timeout;
     xs.drop = a.drop_exchange;
+    xs.armed = false;
     if (threadIdx.x == 0) {
       // peers see the initialised barriers once they have waited on the arrive below
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[0])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&xs.mbar[1])) : "memory");
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    cluster_arrive<CL>();  // matched by the wait of the first exchange
+    // publishes the initialised mbarriers (and, for the passes that start with
+    // a column phase, the free receive blocks); matched by the settle of the first
+    // exchange.  The passes that start with a row phase use the receive blocks as
+    // scratch first and arrive in xchg_rb_done.
+    if constexpr (MODE != kPlaneInit && MODE != kPlaneMulFwd) xchg_arrive<T, Cfg::XCL>(xs);
   }
   grid_dependency_wait();
   const int x = blockIdx.x / CL;
   const int rep = blockIdx.y;
   const int line = threadIdx.x / G, t = threadIdx.x % G;
-  cplx<T>* L = buf + line * LS;
+  // row-phase scratch line: the column line buffer without a cluster or with
+  // direct exchanges, a line of the receive-block region with bulk exchanges
+  cplx<T>* L;
+  if constexpr (Cfg::ALIAS) L = xs.rb + line * LS;
+  else L = buf + line * LS;
   const size_t plane_off = (size_t(rep) * N + x) * FP;
   const size_t real_off = (size_t(rep) * N + x) * size_t(N) * N;
   const int y0 = rank * ROWS + 2 * line;
@@ -746,9 +891,20 @@ plane_kernel(PlaneArgs<T> a) {
       Ops::col_load(buf, a.src + plane_off, rank);
     }
     Ops::col_inverse_to_rows(buf, xs, rank, tw);
-    Ops::row_inverse(v, buf, xs, L, line, t, tw);
+    Ops::row_inverse(v, buf, xs, L, line, t, tw, a.q, DCT && MODE == kPlaneInvReal && a.sin_dz);
     // done with the receive blocks; the step and the adjoint exchange once more
-    if constexpr (MODE == kPlaneStep || MODE == kPlaneAdj || MODE == kPlaneInvMulFwd) cluster_arrive<CL>();
+    if constexpr (MODE == kPlaneInvReal) {
+      if (a.sign_axes) {  // the sine transforms' real-space signs (rows y0, y0 + 1)
+#pragma unroll
+        for (int b = 0; b < E / RL; ++b)
+#pragma unroll
+          for (int r = 0; r < RL; ++r) {
+            const int z = Ops::row_z(t, b, r);
+            v[b * RL + r] = mk<T>(axis_sign<T>(a.sign_axes, x, y0, z) * v[b * RL + r].x,
+                                  axis_sign<T>(a.sign_axes, x, y0 + 1, z) * v[b * RL + r].y);
+          }
+      }
+    }
 
     if (a.flags & (kFlPsiOut | kFlL1 | kFlEnergy)) {
       KahanSum s0, s1, s2;
@@ -859,15 +1015,18 @@ plane_kernel(PlaneArgs<T> a) {
       Ops::col_load(buf, a.src3[c] + plane_off, rank);
       Ops::col_inverse_to_rows(buf, xs, rank, tw);
       Ops::row_inverse(v, buf, xs, L, line, t, tw);
-      cluster_arrive<CL>();  // done with the receive blocks; another exchange follows
+      if (c < 2) xchg_rb_done<T, Cfg::XCL>(xs);  // done with the receive blocks; another exchange follows
       const T* d = a.real_in[1 + c];
 #pragma unroll
       for (int b = 0; b < E / RL; ++b)
 #pragma unroll
         for (int r = 0; r < RL; ++r) {
-          const size_t ia = real_off + size_t(y0) * N + Ops::row_z(t, b, r);
-          acc[b * RL + r].x = fma(v[b * RL + r].x, d[ia], acc[b * RL + r].x);
-          acc[b * RL + r].y = fma(v[b * RL + r].y, d[ia + N], acc[b * RL + r].y);
+          const int z = Ops::row_z(t, b, r);
+          const size_t ia = real_off + size_t(y0) * N + z;
+          // Neumann: the partials carry (-1)^(x+y+z) u (rows y0, y0 + 1)
+          const T sg = axis_sign<T>(a.sign_axes, x, y0, z), sb = axis_sign<T>(a.sign_axes, x, y0 + 1, z);
+          acc[b * RL + r].x = fma(sg * v[b * RL + r].x, d[ia], acc[b * RL + r].x);
+          acc[b * RL + r].y = fma(sb * v[b * RL + r].y, d[ia + N], acc[b * RL + r].y);
         }
     }
     const T beta = T(a.pp.beta), gamma = T(a.pp.gamma);
@@ -887,6 +1046,24 @@ plane_kernel(PlaneArgs<T> a) {
           ob += cpen * (ps[ib - 1] - T(2) * pb + ps[ib + 1]);
         }
         v[b * RL + r] = mk<T>(oa - acc[b * RL + r].x, ob - acc[b * RL + r].y);
+      }
+    Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
+    Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
+  } else if constexpr (MODE == kPlaneMulFwd) {
+    // stress component S_c = (L psi) d_c psi of the Neumann Stokes solve
+    // (cosFFT/comet/morphSurfK.cpp:760-770), signed for the sine transform
+    const T* f0 = a.real_in[0];
+    const T* f1 = a.real_in[1];
+    constexpr int R0 = radix_of<N, -1, 0>();
+#pragma unroll
+    for (int b = 0; b < E / R0; ++b)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int n = in_index<N, -1>(t, b, r);
+        const int z = DCT ? mk_perm<N>(n) : n;
+        const size_t ia = real_off + size_t(y0) * N + z, ib = ia + N;
+        const T sg = axis_sign<T>(a.sign_axes, x, y0, z), sb = axis_sign<T>(a.sign_axes, x, y0 + 1, z);
+        v[b * R0 + r] = mk<T>(sg * f0[ia] * f1[ia], sb * f0[ib] * f1[ib]);
       }
     Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
     Ops::col_forward_store(buf, xs, a.dst + plane_off, rank, tw);
@@ -923,13 +1100,11 @@ plane_kernel(PlaneArgs<T> a) {
         }
       Ops::row_forward_to_cols(v, buf, xs, L, rank, line, t, tw);
       Ops::col_forward_store(buf, xs, (field == 0 ? a.dst2 : a.dst) + plane_off, rank, tw);
-      if (field == 0) cluster_arrive<CL>();  // done with the receive blocks before the second exchange
     }
   }
-  if constexpr (CL > 1) {
-    // outgoing copies must have finished reading this CTA's send blocks
-    if (threadIdx.x < CL) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-  }
+  // every peer has received this CTA's last blocks (and this CTA its own): no
+  // copy still reads its shared memory or is on its way into it
+  xchg_settle<T, Cfg::XCL>(xs);
 }
 
 }  // namespace shb

@@ -74,6 +74,34 @@ __global__ void adj_reduce_kernel(const double* red, int nblocks, double* acc) {
   }
 }
 
+__global__ void shell_argmax_kernel(const double* shell, int nshell, double dq, double* out) {
+  __shared__ double bv[256];
+  __shared__ int bi[256];
+  const double* s = shell + size_t(blockIdx.x) * nshell;
+  double best = -1.0;
+  int idx = 0;
+  for (int i = 1 + threadIdx.x; i < nshell; i += blockDim.x)
+    if (s[i] > best) {  // strided ascending: the first maximum of this thread
+      best = s[i];
+      idx = i;
+    }
+  bv[threadIdx.x] = best;
+  bi[threadIdx.x] = idx;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      const double ov = bv[threadIdx.x + h];
+      const int oi = bi[threadIdx.x + h];
+      if (ov > bv[threadIdx.x] || (ov == bv[threadIdx.x] && oi < bi[threadIdx.x] && oi > 0)) {
+        bv[threadIdx.x] = ov;
+        bi[threadIdx.x] = oi;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = bi[0] * dq;
+}
+
 }  // namespace shb
 
 #define API_CUDA(h, expr)                                                        \
@@ -150,6 +178,7 @@ int sh_default_params(sh_params* p) {
   p->sub_sigma = 0.0;
   p->sub_z0 = 1e-4;
   p->eps_per_replica = nullptr;
+  p->curvature = SH_CURV_DIFFERENCE;
   return SH_OK;
 }
 
@@ -165,13 +194,14 @@ int sh_create(const sh_params* p, sh_handle** out) {
   if (p->scheme != SH_CNAB2 && p->scheme != SH_IMEX_EULER) return fail(nullptr, SH_EINVAL, "bad scheme");
   if (!(p->dx > 0) || !(p->dt > 0)) return fail(nullptr, SH_EINVAL, "dx and dt must be positive");
   if (p->l1_interval < 0) return fail(nullptr, SH_EINVAL, "l1_interval must be >= 0");
-  if (p->advection && p->boundary != SH_PERIODIC)
-    return fail(nullptr, SH_EINVAL, "advection is defined for the periodic boundary only");
   if (p->sub_sigma != 0.0) {
     if (p->boundary != SH_NEUMANN) return fail(nullptr, SH_EUNSUPPORTED, "the substrate penalty is defined for the Neumann boundary");
+    if (p->advection) return fail(nullptr, SH_EUNSUPPORTED, "advection and the substrate penalty are not combined");
     if (!(p->sub_z0 > 0.0)) return fail(nullptr, SH_EINVAL, "sub_z0 must be > 0");
   }
   if (p->variant < 0) return fail(nullptr, SH_EINVAL, "variant must be >= 0");
+  if (p->curvature != SH_CURV_DIFFERENCE && p->curvature != SH_CURV_SPECTRAL)
+    return fail(nullptr, SH_EINVAL, "bad curvature");
 
   SolverBase* s = nullptr;
   const bool f32 = p->precision == SH_FP32;
@@ -346,6 +376,13 @@ int sh_step_async(sh_handle* h, int nsteps) {
   return h->s->step_async(nsteps);
 }
 
+int sh_prepare(sh_handle* h) {
+  ApiRange range_("sh_prepare");
+  if (!h || !h->s) return fail(h, SH_EINVAL, "null handle");
+  if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
+  return h->s->build_graph();
+}
+
 int sh_step(sh_handle* h, int nsteps) {
   ApiRange range_("sh_step");
   int rc = sh_step_async(h, nsteps);
@@ -383,6 +420,20 @@ int sh_energy(sh_handle* h, double* out) {
   return h->s->energy_now(out);
 }
 
+int sh_dominant_wavenumber(sh_handle* h, double* out) {
+  ApiRange range_("sh_dominant_wavenumber");
+  if (!h || !h->s || !out) return fail(h, SH_EINVAL, "null argument");
+  if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
+  return h->s->dominant_wavenumber(out);
+}
+
+int sh_velocity(sh_handle* h, double* ux, double* uy, double* uz) {
+  ApiRange range_("sh_velocity");
+  if (!h || !h->s || !ux || !uy || !uz) return fail(h, SH_EINVAL, "null argument");
+  if (!h->s->ready) return fail(h, SH_ESTATE, "psi was never set");
+  return h->s->velocity(ux, uy, uz);
+}
+
 int sh_energy_trace(sh_handle* h, double* out, int max_steps, int* count) {
   if (!h || !h->s) return fail(h, SH_EINVAL, "null handle");
   SolverBase* s = h->s;
@@ -417,6 +468,20 @@ int sh_adjoint(sh_handle* h, const double* psi0, int nsteps, const double* dl_dp
   int rc = h->s->adjoint(psi0, nsteps, dl_dpsi_t, ckpt_every, g_eps, g_q0, g_psi0);
   if (rc == SH_OK) h->s->ready = true;
   return rc;
+}
+
+int sh_adjoint_forward(sh_handle* h, const double* psi0, int nsteps, int ckpt_every) {
+  ApiRange range_("sh_adjoint_forward");
+  if (!h || !h->s || !psi0) return fail(h, SH_EINVAL, "null argument");
+  int rc = h->s->adjoint_forward(psi0, nsteps, ckpt_every);
+  if (rc == SH_OK) h->s->ready = true;
+  return rc;
+}
+
+int sh_adjoint_backward(sh_handle* h, const double* dl_dpsi_t, double* g_eps, double* g_q0, double* g_psi0) {
+  ApiRange range_("sh_adjoint_backward");
+  if (!h || !h->s || !dl_dpsi_t || !g_eps || !g_q0 || !g_psi0) return fail(h, SH_EINVAL, "null argument");
+  return h->s->adjoint_backward(dl_dpsi_t, g_eps, g_q0, g_psi0);
 }
 
 int sh_checkpoint_save(sh_handle* h, void* buf, size_t* bytes) {

@@ -48,6 +48,7 @@ enum PassFlags : int {
   kFlEnergy = 4,    // plane / pencil: energy partial sums
   kFlRealOut = 8,   // plane step: write psi (T) to real_out
   kFlSpecOut = 16,  // pencil step: write psihat^{n+1} (pencil-major) to spec_out
+  kFlShell = 32,    // pencil energy pass: spectral power per |k| shell into PencilArgs::shell
 };
 
 // Per-launch scalar parameters of the pointwise stages.

@@ -17,35 +17,39 @@ SolverBase* make_if_fits() {
   }
 }
 
-template <typename T, bool DCT>
-SolverBase* make_solver(int n, int variant) {
-  const int cl = variant;
-  switch (n) {
-    case 16: return cl == 0 || cl == 1 ? make_if_fits<T, 16, 1, DCT>() : nullptr;
-    case 32: return cl == 0 || cl == 1 ? make_if_fits<T, 32, 1, DCT>() : nullptr;
-    case 64:
-      if (cl == 0 || cl == 1) return make_if_fits<T, 64, 1, DCT>();
-      if (cl == 2) return make_if_fits<T, 64, 2, DCT>();
-      return nullptr;
-    case 128:
-      if (cl == 0 || cl == 1) return make_if_fits<T, 128, 1, DCT>();
-      if (cl == 2) return make_if_fits<T, 128, 2, DCT>();
-      if (cl == 4) return make_if_fits<T, 128, 4, DCT>();
-      return nullptr;
-    case 256:
-      // default: 8 for FP32 (three CTAs per SM), 16 for FP64 (half the shared
-      // memory of 8, two CTAs per SM)
-      if (cl == 4) return make_if_fits<T, 256, 4, DCT>();
-      if (cl == 8 || (cl == 0 && sizeof(T) == 4)) return make_if_fits<T, 256, 8, DCT>();
-      if (cl == 16 || (cl == 0 && sizeof(T) == 8)) return make_if_fits<T, 256, 16, DCT>();
-      return nullptr;
-#ifdef SHB_WITH_512
-    case 512:
-      if (cl == 0 || cl == 16) return make_if_fits<T, 512, 16, DCT>();
-      return nullptr;
-#endif
-    default: return nullptr;
+// Solver of one grid size N with cluster size ``cl`` (0 = the default).
+template <typename T, int N, bool DCT>
+SolverBase* make_sized(int cl) {
+  if constexpr (N <= 32) {
+    return cl == 0 || cl == 1 ? make_if_fits<T, N, 1, DCT>() : nullptr;
+  } else if constexpr (N == 64) {
+    if (cl == 0 || cl == 1) return make_if_fits<T, 64, 1, DCT>();
+    if (cl == 2) return make_if_fits<T, 64, 2, DCT>();
+    return nullptr;
+  } else if constexpr (N == 128) {
+    if (cl == 0 || cl == 1) return make_if_fits<T, 128, 1, DCT>();
+    if (cl == 2) return make_if_fits<T, 128, 2, DCT>();
+    if (cl == 4) return make_if_fits<T, 128, 4, DCT>();
+    return nullptr;
+  } else if constexpr (N == 256) {
+    // default: 8 for FP32 (three CTAs per SM), 16 for FP64 (half the shared
+    // memory of 8, two CTAs per SM)
+    if (cl == 4) return make_if_fits<T, 256, 4, DCT>();
+    if (cl == 8 || (cl == 0 && sizeof(T) == 4)) return make_if_fits<T, 256, 8, DCT>();
+    if (cl == 16 || (cl == 0 && sizeof(T) == 8)) return make_if_fits<T, 256, 16, DCT>();
+    return nullptr;
+  } else {
+    if (cl == 0 || cl == 16) return make_if_fits<T, 512, 16, DCT>();
+    return nullptr;
   }
 }
 
 }  // namespace shb
+
+// One translation unit per (precision, boundary, size group) so that nvcc
+// compiles them in parallel: SHB_INST_UNIT(f32, neumann, float, true, 256)
+// defines shb::make_solver_f32_neumann_n256.
+#define SHB_INST_UNIT(P, B, T, DCT, N) \
+  namespace shb {                       \
+  SolverBase* make_solver_##P##_##B##_n##N(int cl) { return make_sized<T, N, DCT>(cl); } \
+  }

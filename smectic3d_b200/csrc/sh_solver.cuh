@@ -51,6 +51,15 @@ __global__ void finalize_kernel(const double* red_plane, int nbp, const double* 
 // Sums the per-CTA (eps, q0) gradient slots of the reverse sweep into
 // acc[rep][4] = {g_eps, 0, g_q0, 0}.
 __global__ void adj_reduce_kernel(const double* red, int nblocks, double* acc);
+// dst[i] = double(src[i])
+template <typename T>
+__global__ void to_double_kernel(const T* __restrict__ src, double* __restrict__ dst, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    dst[i] = double(src[i]);
+}
+// out[rep] = dq * (the shell >= 1 of largest power in shell[rep][nshell]; the
+// lowest such shell on a tie)
+__global__ void shell_argmax_kernel(const double* shell, int nshell, double dq, double* out);
 
 struct SolverBase {
   sh_params p{};
@@ -68,6 +77,7 @@ struct SolverBase {
   double* d_scalar = nullptr;  // batch doubles
   double* d_trace = nullptr;   // energy trace of the current chunk
   double* d_amp[2] = {nullptr, nullptr};  // local-amplitude map work fields (allocated on first use)
+  double* d_shell = nullptr;               // spectral power per |k| shell (allocated on first use)
   int trace_cap = 0;
   std::vector<double> energy_trace;  // host copy, steps * batch
   std::vector<double> l1_last;
@@ -92,6 +102,7 @@ struct SolverBase {
     cudaFree(d_trace);
     cudaFree(d_amp[0]);
     cudaFree(d_amp[1]);
+    cudaFree(d_shell);
     for (auto& e : prof_ev)
       if (e) cudaEventDestroy(e);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
@@ -101,6 +112,7 @@ struct SolverBase {
   virtual int setup() = 0;
   virtual int init_from_psi() = 0;     // d_psi holds psi^0
   virtual int step_async(int n) = 0;
+  virtual int build_graph() = 0;       // instantiate the replayed step graph ahead of time
   // per-launch event timing of the two passes (nullptr: off)
   double* prof_ms = nullptr;
   cudaEvent_t prof_ev[3] = {nullptr, nullptr, nullptr};
@@ -111,12 +123,25 @@ struct SolverBase {
   bool use_graphs = true;
   virtual int psi_to_dpsi() = 0;       // current psi -> d_psi
   virtual int energy_now(double* host) = 0;
+  virtual int dominant_wavenumber(double* host) = 0;
+  virtual int velocity(double* ux, double* uy, double* uz) = 0;
   virtual size_t state_bytes() const = 0;
   virtual int save_state(void* host) = 0;
   virtual int load_state(const void* host) = 0;
   virtual int surface_step(int* z, double* vn, double* hh, double* kk) = 0;
-  virtual int adjoint(const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every, double* g_eps,
-                      double* g_q0, double* g_psi0) = 0;
+  // forward sweep from host psi0 keeping a checkpoint every ckpt_every steps,
+  // then (adjoint_backward) the recompute and reverse sweep from those checkpoints
+  virtual int adjoint_forward(const double* psi0, int nsteps, int ckpt_every) = 0;
+  virtual int adjoint_backward(const double* dl_dpsi_t, double* g_eps, double* g_q0, double* g_psi0) = 0;
+  int adjoint(const double* psi0, int nsteps, const double* dl_dpsi_t, int ckpt_every, double* g_eps, double* g_q0,
+              double* g_psi0) {
+    const int rc = adjoint_forward(psi0, nsteps, ckpt_every);
+    return rc ? rc : adjoint_backward(dl_dpsi_t, g_eps, g_q0, g_psi0);
+  }
+  // the checkpoints of the last adjoint_forward, valid while the state is the
+  // one that forward sweep ended in
+  int adj_nsteps = 0, adj_k = 0;
+  long long adj_end = -1;
   virtual int residency(int* out) = 0;
 };
 
@@ -149,8 +174,10 @@ struct Solver final : SolverBase {
   T* Lp = nullptr;
   T* d_wall = nullptr;
   int kwall = 0;
-  // Neumann curvature pass: psi, psi_xx, psi_yy, psi_zz, L psi and a scratch partial
+  // Neumann curvature pass: psi, psi_xx, psi_yy, psi_zz, L psi and a scratch partial;
+  // with the spectral option also psi_x, psi_y, psi_z, psi_xy, psi_xz, psi_yz
   T* CR[5] = {};
+  T* CSP[6] = {};
   cplx<T>* Psc = nullptr;
   bool real_fields_current = false;
   bool u_real_current = false;
@@ -164,10 +191,11 @@ struct Solver final : SolverBase {
     cplx<T>* mp = nullptr;   // partial of c_n mu^{n+1} - mu^{n+2}
     double* red = nullptr;   // per-CTA gradient sums of the reverse sweep
     double* acc = nullptr;
+    cplx<T>* fin = nullptr;  // {W, P, Nt} of the state the forward sweep ended in
     int nseg = 0, k = 0;
     ~AdjBufs() {
       cudaFree(ck); cudaFree(hs); cudaFree(hr); cudaFree(lam); cudaFree(gp); cudaFree(mp);
-      cudaFree(red); cudaFree(acc);
+      cudaFree(red); cudaFree(acc); cudaFree(fin);
     }
   } adj;
   // adjoint: per-step history of a recomputed segment (psihat pencil-major, psi real)
@@ -175,6 +203,7 @@ struct Solver final : SolverBase {
   T* hist_real = nullptr;
   int hist_pos = 0;
   T* q = nullptr;
+  double* qd = nullptr;  // the wavenumbers in FP64 (the FP32 spectral update uses them)
 
   ~Solver() override {
     if (stream) cudaStreamSynchronize(stream);
@@ -183,6 +212,7 @@ struct Solver final : SolverBase {
     cudaFree(Nt);
     cudaFree(tw);
     cudaFree(q);
+    cudaFree(qd);
     cudaFree(Px);
     cudaFree(PSH);
     for (auto* p3 : S3) cudaFree(p3);
@@ -194,6 +224,7 @@ struct Solver final : SolverBase {
     cudaFree(Lp);
     cudaFree(d_wall);
     for (auto* r : CR) cudaFree(r);
+    for (auto* r : CSP) cudaFree(r);
     cudaFree(Psc);
   }
 
@@ -228,21 +259,33 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
+  // a pencil mode whose shared memory does not fit a CTA is never launched
+  template <int MODE>
+  int set_pencil_attrs() {
+    if constexpr (QC::fits(MODE)) return set_attrs(pencil_fn<MODE>(), QC::smem(MODE), false);
+    return SH_OK;
+  }
+
   int setup() override {
     const size_t fe = field_elems();
+    if (p.advection && !QC::fits(kPencilStokes)) {
+      err = "Stokes advection is not built for this size and precision (its pencil pass does not fit a CTA)";
+      return SH_EUNSUPPORTED;
+    }
     SHB_CUDA(dev_malloc(&W, fe * sizeof(cplx<T>)));
     SHB_CUDA(dev_malloc(&P, fe * sizeof(cplx<T>)));
     SHB_CUDA(dev_malloc(&Nt, fe * sizeof(cplx<T>)));
     if (p.advection) {
-      if constexpr (DCT) {
-        err = "advection is defined for the periodic boundary only";
-        return SH_EINVAL;
-      } else {
-        SHB_CUDA(dev_malloc(&Px, fe * sizeof(cplx<T>)));
-        SHB_CUDA(dev_malloc(&PSH, fe * sizeof(cplx<T>)));
-        for (auto& p3 : S3) SHB_CUDA(dev_malloc(&p3, fe * sizeof(cplx<T>)));
-        for (auto& r : R) SHB_CUDA(dev_malloc(&r, size_t(p.batch) * N * N * N * sizeof(T)));
+      // periodic: partials of psi, i q_x psi and opSH psi; Neumann: of psi and
+      // opSH psi (its gradient is a difference stencil in real space)
+      if (DCT && p.sub_sigma != 0.0) {
+        err = "advection and the substrate penalty are not combined";
+        return SH_EUNSUPPORTED;
       }
+      if (!DCT) SHB_CUDA(dev_malloc(&Px, fe * sizeof(cplx<T>)));
+      SHB_CUDA(dev_malloc(&PSH, fe * sizeof(cplx<T>)));
+      for (auto& p3 : S3) SHB_CUDA(dev_malloc(&p3, fe * sizeof(cplx<T>)));
+      for (auto& r : R) SHB_CUDA(dev_malloc(&r, size_t(p.batch) * N * N * N * sizeof(T)));
     }
     if (p.sub_sigma != 0.0) {
       if constexpr (!DCT) {
@@ -266,19 +309,23 @@ struct Solver final : SolverBase {
     }
     SHB_CUDA(dev_malloc(&tw, tw_total<N>() * sizeof(cplx<T>)));
     SHB_CUDA(dev_malloc(&q, N * sizeof(T)));
+    SHB_CUDA(dev_malloc(&qd, N * sizeof(double)));
     SHB_CUDA(dev_malloc(&d_red_plane, size_t(p.batch) * N * CL * 3 * sizeof(double)));
     SHB_CUDA(dev_malloc(&d_red_spec, size_t(p.batch) * QC::TILES * sizeof(double)));
     std::vector<cplx<T>> htw;
     host_twiddles<T, N>(htw);
     std::vector<T> hq(N);
+    std::vector<double> hqd(N);
     if (!DCT) {
       // periodicFFT/pf3d.cpp:166-190 (Nyquist entry +pi/dx)
       for (int i = 0; i < N; ++i)
-        hq[i] = T(i < N / 2 + 1 ? 2.0 * M_PI * i / (p.dx * N) : -(N - i) * 2.0 * M_PI / (p.dx * N));
+        hqd[i] = i < N / 2 + 1 ? 2.0 * M_PI * i / (p.dx * N) : -(N - i) * 2.0 * M_PI / (p.dx * N);
     } else {
       // cosFFT/mesabi/cosNoAdvMorph.cpp:216-231
-      for (int i = 0; i < N; ++i) hq[i] = T(M_PI * i / (p.dx * N));
+      for (int i = 0; i < N; ++i) hqd[i] = M_PI * i / (p.dx * N);
     }
+    for (int i = 0; i < N; ++i) hq[i] = T(hqd[i]);
+    SHB_CUDA(cudaMemcpy(qd, hqd.data(), N * sizeof(double), cudaMemcpyHostToDevice));
     SHB_CUDA(cudaMemcpy(tw, htw.data(), htw.size() * sizeof(cplx<T>), cudaMemcpyHostToDevice));
     SHB_CUDA(cudaMemcpy(q, hq.data(), N * sizeof(T), cudaMemcpyHostToDevice));
     int rc;
@@ -286,20 +333,21 @@ struct Solver final : SolverBase {
     if ((rc = set_attrs(plane_fn<kPlaneInit>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneGetPsi>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneInvReal>(), PC::SMEM, true))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilStep>(), QC::smem(kPencilStep), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilInit>(), QC::smem(kPencilInit), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilEnergy>(), QC::smem(kPencilEnergy), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilStepAdv>(), QC::smem(kPencilStepAdv), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilInitAdv>(), QC::smem(kPencilInitAdv), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilStokes>(), QC::smem(kPencilStokes), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilXMul>(), QC::smem(kPencilXMul), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilSpec>(), QC::smem(kPencilSpec), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilAdjInit>(), QC::smem(kPencilAdjInit), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilAdj>(), QC::smem(kPencilAdj), false))) return rc;
-    if ((rc = set_attrs(pencil_fn<kPencilAdjOut>(), QC::smem(kPencilAdjOut), false))) return rc;
+    if ((rc = set_pencil_attrs<kPencilStep>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilInit>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilEnergy>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilStepAdv>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilInitAdv>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilStokes>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilXMul>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilSpec>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilAdjInit>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilAdj>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilAdjOut>())) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneAdj>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneInvMulFwd>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneAdvN>(), PC::SMEM, true))) return rc;
+    if ((rc = set_attrs(plane_fn<kPlaneMulFwd>(), PC::SMEM, true))) return rc;
     return SH_OK;
   }
 
@@ -397,6 +445,7 @@ struct Solver final : SolverBase {
     PencilArgs<T> a{};
     a.tw = tw;
     a.q = q;
+    a.qd = qd;
     a.pp = point_params();
     a.red = d_red_spec;
     a.nonfinite = d_flag;
@@ -434,6 +483,7 @@ struct Solver final : SolverBase {
 
   int init_from_psi() override {
     int rc;
+    adj_end = -1;
     PlaneArgs<T> a = plane_args();
     a.psi_in = d_psi;
     a.dst2 = P;   // partial of psi^0 (consumed by the init pencil, then overwritten)
@@ -460,10 +510,11 @@ struct Solver final : SolverBase {
     } else {
       if ((rc = launch_plane<kPlaneInit>(a))) return rc;
       if (p.advection) {
-        b.dst_x = Px;
+        b.dst_x = DCT ? nullptr : Px;
         b.dst_sh = PSH;
         if ((rc = launch_pencil<kPencilInitAdv>(b))) return rc;
-        // the first advected N (N-hat^{-1} above discards advection, pf3d.cpp:363-374)
+        // the first advected N (N-hat^{-1} above discards advection, pf3d.cpp:363-374,
+        // cosFFT/comet/morphSurfK.cpp:629-636)
         if ((rc = adv_nonlinear(0))) return rc;
       } else {
         if ((rc = launch_pencil<kPencilInit>(b))) return rc;
@@ -480,26 +531,35 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
+  // plain steps are replayed from a CUDA graph when no per-step host
+  // bookkeeping is needed
+  bool graph_eligible() const {
+    return use_graphs && !prof_ms && !hist_spec && !p.energy_trace && p.l1_interval == 0;
+  }
+  // capture kGraphChunk steps once (nothing runs; the steps counter is restored)
+  int build_graph() override {
+    if (graph_exec || !graph_eligible()) return SH_OK;
+    cudaGraph_t g;
+    const long long s0 = steps, l0 = launches;
+    SHB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    const int rc = step_direct(kGraphChunk);
+    cudaError_t e = cudaStreamEndCapture(stream, &g);
+    steps = s0;
+    hist_pos -= kGraphChunk;
+    graph_launches = launches - l0;
+    launches = l0;
+    if (rc) return rc;
+    SHB_CUDA(e);
+    e = cudaGraphInstantiate(&graph_exec, g, 0);
+    cudaGraphDestroy(g);
+    SHB_CUDA(e);
+    return SH_OK;
+  }
+
   int step_async(int n) override {
-    if (use_graphs && !prof_ms && !hist_spec && !p.energy_trace && p.l1_interval == 0 && n >= kGraphChunk) {
+    if (graph_eligible() && n >= kGraphChunk) {
       int rc;
-      if (!graph_exec) {
-        // capture kGraphChunk steps once; the steps counter is restored after
-        cudaGraph_t g;
-        const long long s0 = steps, l0 = launches;
-        SHB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-        rc = step_direct(kGraphChunk);
-        cudaError_t e = cudaStreamEndCapture(stream, &g);
-        steps = s0;
-        hist_pos -= kGraphChunk;
-        graph_launches = launches - l0;
-        launches = l0;
-        if (rc) return rc;
-        SHB_CUDA(e);
-        e = cudaGraphInstantiate(&graph_exec, g, 0);
-        cudaGraphDestroy(g);
-        SHB_CUDA(e);
-      }
+      if ((rc = build_graph())) return rc;
       const int chunks = n / kGraphChunk;
       for (int c = 0; c < chunks; ++c) {
         SHB_CUDA(cudaGraphLaunch(graph_exec, stream));
@@ -538,7 +598,7 @@ struct Solver final : SolverBase {
       if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[0], stream));
       const int diag = (trace ? kFlEnergy : 0) | (l1_now ? kFlL1 : 0) | (stash_now ? kFlPsiOut : 0);
       if (p.advection) {
-        b.dst_x = Px;
+        b.dst_x = DCT ? nullptr : Px;
         b.dst_sh = PSH;
         if ((rc = launch_pencil<kPencilStepAdv>(b))) return rc;
         if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
@@ -591,7 +651,51 @@ struct Solver final : SolverBase {
   // N = beta psi^3 - gamma psi^5 (+ penalty) - u.grad psi, forward y,z -> Nt.
   int adv_nonlinear(int diag) {
     if constexpr (DCT) {
-      return SH_EINVAL;
+      // Neumann box (cosFFT/comet/morphSurfK.cpp:686-898): psi and L psi to real
+      // space, grad psi by the wall stencil, S_c = (L psi) d_c psi through the
+      // sine transform (signed cosine pair), the projector in the pencil pass,
+      // then N = beta psi^3 - gamma psi^5 - u . grad psi forward -> Nt
+      int rc;
+      const cplx<T>* src[2] = {P, PSH};
+      const int out[2] = {0, 4};
+      for (int i = 0; i < 2; ++i) {
+        PlaneArgs<T> a = plane_args();
+        a.src = src[i];
+        a.real_out = R[out[i]];
+        if (i == 0) {
+          a.flags = diag;
+          a.psi_old = d_stash;
+          a.psi_out = d_stash;
+        }
+        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      }
+      grad_wall_kernel<T><<<dim3(4 * 148, p.batch), 256, 0, stream>>>(R[0], R[1], R[2], R[3], N,
+                                                                        T(0.5 / p.dx));
+      SHB_CUDA(cudaGetLastError());
+      ++launches;
+      for (int c = 0; c < 3; ++c) {
+        PlaneArgs<T> a = plane_args();
+        a.real_in[0] = R[4];
+        a.real_in[1] = R[1 + c];
+        a.sign_axes = 7;
+        a.dst = S3[c];
+        if ((rc = launch_plane<kPlaneMulFwd>(a))) return rc;
+      }
+      PencilArgs<T> b = pencil_args();
+      for (int c = 0; c < 3; ++c) {
+        b.s3[c] = S3[c];
+        b.u3[c] = S3[c];
+      }
+      if ((rc = launch_pencil<kPencilStokes>(b))) return rc;
+      PlaneArgs<T> a = plane_args();
+      for (int i = 0; i < 4; ++i) a.real_in[i] = R[i];
+      for (int c = 0; c < 3; ++c) a.src3[c] = S3[c];
+      a.sign_axes = 7;
+      a.dst = Nt;
+      if ((rc = launch_plane<kPlaneAdvN>(a))) return rc;
+      real_fields_current = true;
+      u_real_current = false;
+      return SH_OK;
     } else {
       int rc;
       // psi and L psi to real space
@@ -644,9 +748,32 @@ struct Solver final : SolverBase {
       PlaneArgs<T> a = plane_args();
       a.src = S3[c];
       a.real_out = R[5 + c];
+      a.sign_axes = DCT ? 7 : 0;  // Neumann: the partials carry (-1)^(x+y+z) u
       if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
     }
     u_real_current = true;
+    return SH_OK;
+  }
+
+  // Stokes velocity of the current state in FP64 (batch * N^3 per component)
+  int velocity(double* ux, double* uy, double* uz) override {
+    if (!p.advection) {
+      err = "the velocity is computed by advected handles (advection = 1)";
+      return SH_EINVAL;
+    }
+    int rc;
+    if (!real_fields_current && (rc = adv_nonlinear(0))) return rc;
+    if (!u_real_current && (rc = velocity_real())) return rc;
+    const size_t nr = size_t(p.batch) * N * N * N;
+    double* outs[3] = {ux, uy, uz};
+    for (int c = 0; c < 3; ++c) {
+      to_double_kernel<T><<<4 * 148, 256, 0, stream>>>(R[5 + c], d_psi, (long long)nr);
+      SHB_CUDA(cudaGetLastError());
+      ++launches;
+      SHB_CUDA(cudaMemcpyAsync(outs[c], d_psi, nr * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      SHB_CUDA(cudaStreamSynchronize(stream));
+    }
+    psi0_valid = false;  // d_psi was used as scratch
     return SH_OK;
   }
 
@@ -677,6 +804,28 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
+  // |q| of the shell holding the most spectral power of the current state,
+  // DC excluded (the dominant layer wavenumber): one pencil pass over the
+  // partial P that builds the per-shell power in FP64, then an argmax per replica
+  int dominant_wavenumber(double* host) override {
+    int rc;
+    const size_t nb = size_t(p.batch) * QC::NSHELL;
+    if (!d_shell) SHB_CUDA(dev_malloc(&d_shell, nb * sizeof(double)));
+    SHB_CUDA(cudaMemsetAsync(d_shell, 0, nb * sizeof(double), stream));
+    PencilArgs<T> b = pencil_args();
+    b.src = P;
+    b.flags = kFlShell;
+    b.shell = d_shell;
+    if ((rc = launch_pencil<kPencilEnergy>(b))) return rc;
+    const double dq = (DCT ? M_PI : 2.0 * M_PI) / (double(N) * p.dx);
+    shell_argmax_kernel<<<p.batch, 256, 0, stream>>>(d_shell, QC::NSHELL, dq, d_scalar);
+    SHB_CUDA(cudaGetLastError());
+    ++launches;
+    SHB_CUDA(cudaMemcpyAsync(host, d_scalar, p.batch * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    SHB_CUDA(cudaStreamSynchronize(stream));
+    return SH_OK;
+  }
+
   size_t state_bytes() const override { return (p.advection ? 5 : 3) * field_elems() * sizeof(cplx<T>); }
   int save_state(void* host) override {
     const size_t fb = field_elems() * sizeof(cplx<T>);
@@ -692,6 +841,7 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
   int load_state(const void* host) override {
+    adj_end = -1;
     const size_t fb = field_elems() * sizeof(cplx<T>);
     const char* h = static_cast<const char*>(host);
     SHB_CUDA(cudaMemcpyAsync(W, h, fb, cudaMemcpyHostToDevice, stream));
@@ -713,8 +863,8 @@ struct Solver final : SolverBase {
   // c_n = 3, c_0 = 2) for a loss whose gradient with respect to psi^T is
   // dl_dpsi_t.  The forward states are checkpointed every ckpt_every steps and
   // recomputed segment by segment; the (eps, q0) gradients accumulate in FP64.
-  int adjoint(const double* psi0, int nsteps, const double* dl_dpsi_t, int K, double* g_eps, double* g_q0,
-              double* g_psi0) override {
+  // the adjoint covers the plain periodic CNAB2 step
+  int adjoint_supported() {
     if constexpr (DCT) {
       err = "the adjoint is built for the periodic boundary";
       return SH_EUNSUPPORTED;
@@ -723,20 +873,10 @@ struct Solver final : SolverBase {
         err = "the adjoint covers the plain CNAB2 step without advection or penalty";
         return SH_EUNSUPPORTED;
       }
-      if (nsteps < 1 || K < 1) {
-        err = "nsteps and ckpt_every must be >= 1";
-        return SH_EINVAL;
-      }
-      int rc;
-      const size_t fe = field_elems();
-      const size_t nr = size_t(p.batch) * N * N * N;
-      const int nseg = (nsteps + K - 1) / K;
-      const bool saved_trace = p.energy_trace != 0;
-      const int saved_l1 = p.l1_interval;
-      p.energy_trace = 0;
-      p.l1_interval = 0;
-      AdjBufs& bf = adj;
-      auto restore = [&]() { p.energy_trace = saved_trace; p.l1_interval = saved_l1; hist_spec = nullptr; hist_real = nullptr; };
+      return SH_OK;
+    }
+  }
+
 #define ADJ_CUDA(expr)                                                           \
   do {                                                                           \
     cudaError_t e_ = (expr);                                                     \
@@ -753,14 +893,78 @@ struct Solver final : SolverBase {
       return rc;           \
     }                      \
   } while (0)
-      // buffers persist across calls; they grow when nsteps / ckpt_every need more
-      if (bf.nseg < nseg) {
-        cudaFree(bf.ck);
-        bf.ck = nullptr;
-        bf.nseg = 0;
-        ADJ_CUDA(dev_malloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
-        bf.nseg = nseg;
+
+  // Forward sweep of the discrete adjoint: psi0 from the host, nsteps plain
+  // steps, a checkpoint (W, P, Nt) at s = 0, K, 2K, ...  The handle then holds
+  // psi^T as after sh_run, and adjoint_backward can use the checkpoints.
+  int adjoint_forward(const double* psi0, int nsteps, int K) override {
+    int rc;
+    if ((rc = adjoint_supported())) return rc;
+    if (nsteps < 1 || K < 1) {
+      err = "nsteps and ckpt_every must be >= 1";
+      return SH_EINVAL;
+    }
+    const size_t fe = field_elems();
+    const size_t nr = size_t(p.batch) * N * N * N;
+    const int nseg = (nsteps + K - 1) / K;
+    const bool saved_trace = p.energy_trace != 0;
+    const int saved_l1 = p.l1_interval;
+    p.energy_trace = 0;
+    p.l1_interval = 0;
+    AdjBufs& bf = adj;
+    auto restore = [&]() { p.energy_trace = saved_trace; p.l1_interval = saved_l1; };
+    // buffers persist across calls; they grow when nsteps / ckpt_every need more
+    if (bf.nseg < nseg) {
+      cudaFree(bf.ck);
+      bf.ck = nullptr;
+      bf.nseg = 0;
+      ADJ_CUDA(dev_malloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
+      bf.nseg = nseg;
+    }
+    const size_t fb = fe * sizeof(cplx<T>);
+    ADJ_CUDA(cudaMemcpyAsync(d_psi, psi0, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
+    ADJ_RC(init_from_psi());
+    for (int sg = 0; sg < nseg; ++sg) {
+      cplx<T>* c = bf.ck + size_t(sg) * 3 * fe;
+      ADJ_CUDA(cudaMemcpyAsync(c, W, fb, cudaMemcpyDeviceToDevice, stream));
+      ADJ_CUDA(cudaMemcpyAsync(c + fe, P, fb, cudaMemcpyDeviceToDevice, stream));
+      ADJ_CUDA(cudaMemcpyAsync(c + 2 * fe, Nt, fb, cudaMemcpyDeviceToDevice, stream));
+      const int s1 = (sg + 1) * K < nsteps ? (sg + 1) * K : nsteps;
+      ADJ_RC(step_async(s1 - sg * K));
+    }
+    restore();
+    psi0_valid = false;
+    adj_nsteps = nsteps;
+    adj_k = K;
+    adj_end = steps;
+    return SH_OK;
+  }
+
+  // Reverse sweep from the checkpoints of the last adjoint_forward (the
+  // handle must still hold the state that sweep ended in): lambda^T from
+  // dl_dpsi_t, then per segment in reverse the recomputed states and the
+  // adjoint steps.  Leaves the handle's state at psi^T.
+  int adjoint_backward(const double* dl_dpsi_t, double* g_eps, double* g_q0, double* g_psi0) override {
+    if constexpr (DCT) {
+      return adjoint_supported();
+    } else {
+      int rc;
+      if ((rc = adjoint_supported())) return rc;
+      if (adj_end < 0 || adj_end != steps) {
+        err = "no forward sweep with checkpoints ends at the current state (call sh_adjoint_forward first)";
+        return SH_ESTATE;
       }
+      const int nsteps = adj_nsteps, K = adj_k;
+      const size_t fe = field_elems();
+      const size_t nr = size_t(p.batch) * N * N * N;
+      const int nseg = (nsteps + K - 1) / K;
+      const bool saved_trace = p.energy_trace != 0;
+      const int saved_l1 = p.l1_interval;
+      p.energy_trace = 0;
+      p.l1_interval = 0;
+      AdjBufs& bf = adj;
+      // the state at psi^T, restored at the end: the last checkpoint's segment is recomputed over it
+      auto restore = [&]() { p.energy_trace = saved_trace; p.l1_interval = saved_l1; hist_spec = nullptr; hist_real = nullptr; };
       if (bf.k < K) {
         cudaFree(bf.hs);
         cudaFree(bf.hr);
@@ -777,20 +981,15 @@ struct Solver final : SolverBase {
         ADJ_CUDA(dev_malloc(&bf.mp, fe * sizeof(cplx<T>)));
         ADJ_CUDA(dev_malloc(&bf.red, size_t(p.batch) * QC::TILES * 2 * sizeof(double)));
         ADJ_CUDA(dev_malloc(&bf.acc, size_t(p.batch) * 4 * sizeof(double)));
+        ADJ_CUDA(dev_malloc(&bf.fin, 3 * fe * sizeof(cplx<T>)));
       }
       ADJ_CUDA(cudaMemsetAsync(bf.red, 0, size_t(p.batch) * QC::TILES * 2 * sizeof(double), stream));
       const size_t fb = fe * sizeof(cplx<T>);
-      // ---- forward sweep with checkpoints at s = 0, K, 2K, ...
-      ADJ_CUDA(cudaMemcpyAsync(d_psi, psi0, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
-      ADJ_RC(init_from_psi());
-      for (int sg = 0; sg < nseg; ++sg) {
-        cplx<T>* c = bf.ck + size_t(sg) * 3 * fe;
-        ADJ_CUDA(cudaMemcpyAsync(c, W, fb, cudaMemcpyDeviceToDevice, stream));
-        ADJ_CUDA(cudaMemcpyAsync(c + fe, P, fb, cudaMemcpyDeviceToDevice, stream));
-        ADJ_CUDA(cudaMemcpyAsync(c + 2 * fe, Nt, fb, cudaMemcpyDeviceToDevice, stream));
-        const int s1 = (sg + 1) * K < nsteps ? (sg + 1) * K : nsteps;
-        ADJ_RC(step_async(s1 - sg * K));
-      }
+      const long long end_steps = steps;
+      // keep the final state (the recompute overwrites W, P, Nt)
+      ADJ_CUDA(cudaMemcpyAsync(bf.fin, W, fb, cudaMemcpyDeviceToDevice, stream));
+      ADJ_CUDA(cudaMemcpyAsync(bf.fin + fe, P, fb, cudaMemcpyDeviceToDevice, stream));
+      ADJ_CUDA(cudaMemcpyAsync(bf.fin + 2 * fe, Nt, fb, cudaMemcpyDeviceToDevice, stream));
       // ---- lambda^T -> lambdahat^T and the partial of mu^T = B lambda^T
       ADJ_CUDA(cudaMemcpyAsync(d_psi, dl_dpsi_t, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
       {
@@ -866,24 +1065,34 @@ struct Solver final : SolverBase {
       std::vector<double> acc(size_t(p.batch) * 4);
       ADJ_CUDA(cudaMemcpyAsync(acc.data(), bf.acc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
       ADJ_CUDA(cudaMemcpyAsync(g_psi0, d_psi, nr * sizeof(double), cudaMemcpyDeviceToHost, stream));
+      // back to the state the forward sweep ended in
+      ADJ_CUDA(cudaMemcpyAsync(W, bf.fin, fb, cudaMemcpyDeviceToDevice, stream));
+      ADJ_CUDA(cudaMemcpyAsync(P, bf.fin + fe, fb, cudaMemcpyDeviceToDevice, stream));
+      ADJ_CUDA(cudaMemcpyAsync(Nt, bf.fin + 2 * fe, fb, cudaMemcpyDeviceToDevice, stream));
       ADJ_CUDA(cudaStreamSynchronize(stream));
       for (int r = 0; r < p.batch; ++r) {
         g_eps[r] = acc[size_t(r) * 4 + 0];
         g_q0[r] = acc[size_t(r) * 4 + 2];
       }
+      steps = end_steps;
       psi0_valid = false;
       restore();
-#undef ADJ_CUDA
-#undef ADJ_RC
       return SH_OK;
     }
   }
+#undef ADJ_CUDA
+#undef ADJ_RC
 
   // surfTrack pass (periodicFFT/surfTrack.cpp:592-626, 744-806): one advected
   // step; the crossing of psi^{n+1} per (x, y) column with v_n, H, K from the
   // fields of state n.
   int surface_step(int* z, double* vn, double* hh, double* kk) override {
     if constexpr (DCT) {
+      if (p.advection) {
+        // d_t psi of cosNoAdvMorphCurv has no u . grad psi term
+        err = "the Neumann curvature pass is defined for handles without advection";
+        return SH_EUNSUPPORTED;
+      }
       // curvature pass of cosFFT/comet/cosNoAdvMorphCurv.cpp:742-965 at state n, then one step
       int rc;
       const size_t nr = size_t(p.batch) * N * N * N, nc = size_t(p.batch) * N * N;
@@ -892,6 +1101,32 @@ struct Solver final : SolverBase {
         SHB_CUDA(dev_malloc(&Psc, field_elems() * sizeof(cplx<T>)));
         SHB_CUDA(dev_malloc(&d_zout, nc * sizeof(int)));
         for (auto& d : d_surf) SHB_CUDA(dev_malloc(&d, nc * sizeof(double)));
+      }
+      CurvArgs<T> ca{};
+      if (p.curvature == SH_CURV_SPECTRAL) {
+        // exact first and mixed derivatives of the cosine series: d/dx, d/dy, d/dz
+        // turn the cosine series along that axis into a sine series, inverted as the
+        // REDFT01 of reversed coefficients times (-1)^index (sign_axes)
+        if (!CSP[0])
+          for (auto& r : CSP) SHB_CUDA(dev_malloc(&r, nr * sizeof(T)));
+        PencilArgs<T> b = pencil_args();
+        b.src = P;
+        b.dst = Psc;
+        b.xmul = kXSinDx;
+        if ((rc = launch_pencil<kPencilXMul>(b))) return rc;
+        struct D { const cplx<T>* src; int mult, sin_dz, sign; };
+        const D d[6] = {{Psc, kMulNone, 0, 1}, {P, kMulSinDy, 0, 2}, {P, kMulNone, 1, 4},
+                        {Psc, kMulSinDy, 0, 3}, {Psc, kMulNone, 1, 5}, {P, kMulSinDy, 1, 6}};
+        for (int i = 0; i < 6; ++i) {
+          PlaneArgs<T> a = plane_args();
+          a.src = d[i].src;
+          a.mult = d[i].mult;
+          a.sin_dz = d[i].sin_dz;
+          a.sign_axes = d[i].sign;
+          a.real_out = CSP[i];
+          if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+          ca.spec[i] = CSP[i];
+        }
       }
       // psi, psi_yy, psi_zz from the partial of psi; psi_xx and L psi through an x multiplier
       const int mult[3] = {kMulNone, kMulNegQy2, kMulNegQz2};
@@ -916,7 +1151,6 @@ struct Solver final : SolverBase {
         a.real_out = xo[i];
         if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
       }
-      CurvArgs<T> ca;
       ca.psi = CR[0];
       ca.dxx = CR[1];
       ca.dyy = CR[2];
@@ -1004,10 +1238,30 @@ struct Solver final : SolverBase {
   }
 };
 
-// factory: defined per precision / boundary in the instantiation units
-SolverBase* make_solver_f32_periodic(int n, int variant);
-SolverBase* make_solver_f64_periodic(int n, int variant);
-SolverBase* make_solver_f32_neumann(int n, int variant);
-SolverBase* make_solver_f64_neumann(int n, int variant);
+// factories: one per (precision, boundary, size), defined in the
+// instantiation units sh_inst_<precision>_<boundary>_<size>.cu
+#define SHB_DECLARE_FACTORIES(P, B)                                                                  \
+  SolverBase* make_solver_##P##_##B##_n16(int cl);                                                   \
+  SolverBase* make_solver_##P##_##B##_n32(int cl);                                                   \
+  SolverBase* make_solver_##P##_##B##_n64(int cl);                                                   \
+  SolverBase* make_solver_##P##_##B##_n128(int cl);                                                  \
+  SolverBase* make_solver_##P##_##B##_n256(int cl);                                                  \
+  SolverBase* make_solver_##P##_##B##_n512(int cl);                                                  \
+  inline SolverBase* make_solver_##P##_##B(int n, int variant) {                                     \
+    switch (n) {                                                                                      \
+      case 16: return make_solver_##P##_##B##_n16(variant);                                          \
+      case 32: return make_solver_##P##_##B##_n32(variant);                                          \
+      case 64: return make_solver_##P##_##B##_n64(variant);                                          \
+      case 128: return make_solver_##P##_##B##_n128(variant);                                        \
+      case 256: return make_solver_##P##_##B##_n256(variant);                                        \
+      case 512: return make_solver_##P##_##B##_n512(variant);                                        \
+      default: return nullptr;                                                                        \
+    }                                                                                                 \
+  }
+SHB_DECLARE_FACTORIES(f32, periodic)
+SHB_DECLARE_FACTORIES(f64, periodic)
+SHB_DECLARE_FACTORIES(f32, neumann)
+SHB_DECLARE_FACTORIES(f64, neumann)
+#undef SHB_DECLARE_FACTORIES
 
 }  // namespace shb

@@ -23,6 +23,29 @@
 
 namespace shb {
 
+// Gradient of psi on the Neumann box by centred differences, one-sided at the
+// walls: (psi[i+1] - psi[i-1]) / 2dx inside, 2 (psi[1] - psi[0]) / 2dx and
+// 2 (psi[N-1] - psi[N-2]) / 2dx at the walls, in x, y and z
+// (cosFFT/comet/morphSurfK.cpp:700-766).  One thread per point, replicas in y.
+template <typename T>
+__global__ void grad_wall_kernel(const T* __restrict__ psi, T* __restrict__ gx, T* __restrict__ gy,
+                                 T* __restrict__ gz, int n, T inv2dx) {
+  const long long n3 = (long long)n * n * n, nn = (long long)n * n;
+  const size_t off = size_t(blockIdx.y) * n3;
+  const T* p = psi + off;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x) {
+    const int z = int(i % n), y = int((i / n) % n), x = int(i / nn);
+    auto diff = [&](int c, long long s) {
+      if (c == 0) return T(2) * (p[i + s] - p[i]) * inv2dx;
+      if (c == n - 1) return T(2) * (p[i] - p[i - s]) * inv2dx;
+      return (p[i + s] - p[i - s]) * inv2dx;
+    };
+    gx[off + i] = diff(x, nn);
+    gy[off + i] = diff(y, n);
+    gz[off + i] = diff(z, 1);
+  }
+}
+
 template <typename T>
 struct SurfArgs {
   const T* psi;      // state n
@@ -114,6 +137,9 @@ struct CurvArgs {
   double* vn;
   double* hh;
   double* kk;
+  // optional exact derivatives of the cosine series: psi_x, psi_y, psi_z,
+  // psi_xy, psi_xz, psi_yz (in place of the differences; all or none)
+  const T* spec[6];
 };
 
 // centred difference along one axis (stride s, index i of n), one-sided at the walls
@@ -153,9 +179,10 @@ __global__ void curv_scan_kernel(CurvArgs<T> a) {
   }
   const double td = 2.0 * a.dx;
   const size_t at = base + k2;
-  const double gx = curv_grad(psi, at, sx, i, n, td);
-  const double gy = curv_grad(psi, at, sy, j, n, td);
-  const double gz = curv_grad(psi, at, 1, k2, n, td);
+  const bool spec = a.spec[0] != nullptr;
+  const double gx = spec ? double(a.spec[0][at]) : curv_grad(psi, at, sx, i, n, td);
+  const double gy = spec ? double(a.spec[1][at]) : curv_grad(psi, at, sy, j, n, td);
+  const double gz = spec ? double(a.spec[2][at]) : curv_grad(psi, at, 1, k2, n, td);
   const double g = sqrt(gx * gx + gy * gy + gz * gz);
   // psi_xy: y difference of the x gradient at k2
   double dxy;
@@ -183,6 +210,11 @@ __global__ void curv_scan_kernel(CurvArgs<T> a) {
     const double c = (zp - zm == 2) ? 1.0 : 2.0;
     dxz = c * (curv_grad(psi, base + zp, sx, i, n, td) - curv_grad(psi, base + zm, sx, i, n, td)) / td;
     dyz = c * (curv_grad(psi, base + zp, sy, j, n, td) - curv_grad(psi, base + zm, sy, j, n, td)) / td;
+  }
+  if (spec) {
+    dxy = a.spec[3][at];
+    dxz = a.spec[4][at];
+    dyz = a.spec[5][at];
   }
   const double xx = a.dxx[at], yy = a.dyy[at], zz = a.dzz[at];
   const double p = psi[at];

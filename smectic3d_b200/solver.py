@@ -42,6 +42,7 @@ class Params:
     sub_z0: float = 1e-4
     eps_per_replica: tuple | None = None
     variant: int = 0                 # plane-pass cluster size (0 = default, -1 = autotune)
+    curvature: str = "difference"    # Neumann curvature pass: "difference" (reference) | "spectral"
 
     @staticmethod
     def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":
@@ -59,6 +60,7 @@ class Params:
         p.l1_interval = self.l1_interval
         p.energy_trace = int(bool(self.energy_trace))
         p.variant = int(self.variant)
+        p.curvature = {"difference": L.SH_CURV_DIFFERENCE, "spectral": L.SH_CURV_SPECTRAL}[self.curvature]
         for k in ("dx", "dt", "eps", "beta", "gamma", "alpha", "q0", "eta", "rho", "w_mid", "sub_sigma", "sub_z0"):
             setattr(p, k, float(getattr(self, k)))
         keep = None
@@ -131,6 +133,10 @@ class Solver:
     def step_async(self, nsteps: int = 1):
         self._chk(self.lib.sh_step_async(self.h, int(nsteps)))
 
+    def prepare(self):
+        """Instantiate the replayed step graph now (runs nothing)."""
+        self._chk(self.lib.sh_prepare(self.h))
+
     def run(self, psi0: np.ndarray, nsteps: int, out: np.ndarray | None = None) -> np.ndarray:
         a = np.ascontiguousarray(psi0, dtype=np.float64)
         if out is None:
@@ -176,6 +182,18 @@ class Solver:
         out = np.empty(self.params.batch, dtype=np.float64)
         self._chk(self.lib.sh_energy(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
+
+    def dominant_wavenumber(self) -> np.ndarray:
+        """|q| of the spectral shell with the most power, per replica."""
+        out = np.empty(self.params.batch, dtype=np.float64)
+        self._chk(self.lib.sh_dominant_wavenumber(self.h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def velocity(self):
+        """(u_x, u_y, u_z) of the current state of an advected handle."""
+        out = [np.empty(self.shape, dtype=np.float64) for _ in range(3)]
+        self._chk(self.lib.sh_velocity(self.h, *(o.ctypes.data for o in out)))
+        return tuple(out)
 
     def energy_trace(self) -> np.ndarray:
         cnt = C.c_int()
@@ -228,6 +246,24 @@ class Solver:
         self._chk(self.lib.sh_adjoint(self.h, a.ctypes.data, int(nsteps), g.ctypes.data, int(ckpt_every),
                                       ge.ctypes.data_as(C.POINTER(C.c_double)),
                                       gq.ctypes.data_as(C.POINTER(C.c_double)), gp.ctypes.data))
+        return ge, gq, gp
+
+    def adjoint_forward(self, psi0: np.ndarray, nsteps: int, ckpt_every: int = 50):
+        """nsteps steps from psi0 keeping the adjoint's checkpoints; the handle
+        is left at psi^T (read it with get_psi)."""
+        a = np.ascontiguousarray(psi0, dtype=np.float64)
+        self._chk(self.lib.sh_adjoint_forward(self.h, a.ctypes.data, int(nsteps), int(ckpt_every)))
+
+    def adjoint_backward(self, dl_dpsi_t: np.ndarray):
+        """Reverse sweep from the checkpoints of the last adjoint_forward:
+        (dL/d eps, dL/d q0, dL/d psi0) per replica."""
+        g = np.ascontiguousarray(dl_dpsi_t, dtype=np.float64)
+        b = self.params.batch
+        ge = np.empty(b, dtype=np.float64)
+        gq = np.empty(b, dtype=np.float64)
+        gp = np.empty(self.shape, dtype=np.float64)
+        self._chk(self.lib.sh_adjoint_backward(self.h, g.ctypes.data, ge.ctypes.data_as(C.POINTER(C.c_double)),
+                                               gq.ctypes.data_as(C.POINTER(C.c_double)), gp.ctypes.data))
         return ge, gq, gp
 
     def checkpoint(self) -> bytes:

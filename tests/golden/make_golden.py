@@ -1,6 +1,7 @@
 """Generate the golden vectors under tests/golden/ from the FP64 oracle.
 
-    python -m tests.golden.make_golden
+    python -m tests.golden.make_golden            # the small cases
+    python -m tests.golden.make_golden --full     # the measurement configurations (about 25 min)
 
 Each case stores its inputs (psi0, parameters) and the oracle's outputs, so
 the GPU parity tests compare against fixed numbers that do not depend on the
@@ -151,7 +152,54 @@ CASES = {
 }
 
 
-def main():
+def full_case(name: str) -> dict:
+    """A measurement configuration at its own size and length (full_configs.py):
+    the oracle state after each check step, subsampled, with its global sums,
+    energy and dominant wavenumber; for the advected cases also the surfTrack
+    pass of one more step on a subsample of the columns."""
+    from tests.golden import full_configs as F
+    cfg = F.CASES[name]
+    n, stride = cfg["n"], cfg["stride"]
+    p = O.Params(n=n, dx=F.DX, dt=cfg["dt"], eps=cfg.get("eps", -0.75))
+    psi0 = F.initial_condition(cfg)
+    neumann = cfg["boundary"] == "neumann"
+    advect = bool(cfg.get("advect", False))
+    orc = O.NeumannOracle(psi0, p) if neumann else O.PeriodicOracle(psi0, p, advect=advect)
+    efun = O.energy_spectral_neumann if neumann else O.energy_spectral_periodic
+    qfun = O.dominant_wavenumber_neumann if neumann else O.dominant_wavenumber
+    out = {"checks": np.asarray(cfg["checks"]), "energy_0": efun(psi0, p)}
+    done = 0
+    for c in cfg["checks"]:
+        orc.run(c - done)
+        done = c
+        psi = orc.psi
+        out[f"psi_sub_{c}"] = F.subsample(psi, stride)
+        out[f"sum_sq_{c}"] = float(np.sum(psi * psi))
+        out[f"sum_abs_{c}"] = float(np.sum(np.abs(psi)))
+        out[f"energy_{c}"] = efun(psi, p)
+        out[f"qstar_{c}"] = qfun(psi, p.dx)
+    if advect:
+        orc.step()
+        z, vn, hh, kk = O.surface_scan_vec(orc.psi, *orc.surface_fields())
+        ss = cfg["surf_stride"]
+        out.update(surf_z=z[::ss, ::ss], surf_vn=vn[::ss, ::ss], surf_h=hh[::ss, ::ss], surf_k=kk[::ss, ::ss],
+                   psi_sub_surface=F.subsample(orc.psi, stride))
+    return _pack(p, **out)
+
+
+def full_path(name: str) -> str:
+    return path("full_" + name)
+
+
+def main(argv=None):
+    import sys
+    argv = sys.argv[1:] if argv is None else argv
+    if argv and argv[0] == "--full":
+        from tests.golden import full_configs as F
+        for name in argv[1:] or list(F.CASES):
+            np.savez_compressed(full_path(name), **full_case(name))
+            print("wrote", full_path(name), flush=True)
+        return
     for name, fn in CASES.items():
         np.savez_compressed(path(name), **fn())
         print("wrote", path(name))

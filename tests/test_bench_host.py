@@ -115,6 +115,8 @@ def test_reference_arm_rank0_prints_one_line_other_ranks_nothing():
     assert d["cpu_baseline"]["kind"] == "port" and d["cpu_baseline"]["value"] == d["value"]
     assert d["e2e"] == {"value": d["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert d["higher_is_better"] is True and d["metric"] == bench.METRIC
+    # the arm runs the warm-up and timed steps it was asked for
+    assert d["steps"] == 1 and d["warmup"] == 3
 
 
 def test_warmup_below_three_is_refused():

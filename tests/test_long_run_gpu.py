@@ -1,0 +1,70 @@
+"""Long runs: the dominant layer wavenumber and the energy over 2000 steps.
+
+The FP64 path is pinned to the oracle over 2000 steps by the 64^3 fixtures of
+test_full_configs_gpu.py (energy to 1e-10, the same dominant shell).  Here the
+FP32 path (FP32 fields and transforms, FP64 energy sums and FP64 CNAB2
+multipliers) runs beside the FP64 path at the measurement sizes:
+
+* C2 (Neumann 256^3, the 0.5 hyperboloid, which decays by 60 orders of
+  magnitude over 2000 steps) and C2' (amplitude 1.328, which does not);
+* C4 (64 replicas of 64^3 with eps from -0.9 to -0.5, decaying noise) and C4'
+  (1.328 cos(z) lamellae plus that noise in every replica).
+
+The dominant wavenumber must be the same shell in every run.  The energy is
+compared with the bound written beside each case: on a decaying field the FP32
+rounding of each step accumulates in the relative error of the surviving modes,
+and replica 0 of C4' sits at eps = -0.9, the saddle-node of the lamellar branch
+(eps + 3/4 beta A^2 - 5/8 gamma A^4 = 0 has a double root there), where the
+dynamics amplify any rounding difference; its wavenumber still agrees.
+"""
+import numpy as np
+import pytest
+
+import smectic3d_b200 as S
+from tests.golden import full_configs as F
+
+pytestmark = pytest.mark.gpu
+
+CHECKS = (100, 500, 1000, 2000)
+
+
+def run(p, psi0):
+    out = []
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        done = 0
+        for c in CHECKS:
+            s.step(c - done)
+            done = c
+            out.append((s.energy(), s.dominant_wavenumber()))
+    return out
+
+
+@pytest.mark.parametrize("amp,etol", [(0.5, 1e-4), (1.328, 5e-6)])
+def test_c2_long_run_fp32_against_fp64(amp, etol):
+    psi0 = S.ic.hyperboloid(256, F.DX, amp=amp, seed=0)
+    res = {prec: run(S.Params(n=256, boundary="neumann", precision=prec, dt=0.05, eps=-0.75), psi0)
+           for prec in ("fp64", "fp32")}
+    for c, (e64, q64), (e32, q32) in zip(CHECKS, res["fp64"], res["fp32"]):
+        assert q32[0] == q64[0], (c, q32, q64)
+        rel = abs(e32[0] - e64[0]) / abs(e64[0])
+        print(f"C2 amp {amp} step {c}: q* {q64[0]:.6f}, energy rel err FP32 vs FP64 {rel:.3e}")
+        assert rel <= etol, (c, rel)
+
+
+@pytest.mark.parametrize("lamellae,etol", [(False, 5e-4), (True, 1e-6)])
+def test_c4_long_run_fp32_against_fp64(lamellae, etol):
+    b = 64
+    eps = tuple(np.linspace(-0.9, -0.5, b))
+    psi0 = S.ic.noise_batch(64, range(b))
+    if lamellae:
+        psi0 = psi0 + 1.328 * np.cos(np.arange(64) * F.DX)[None, None, None, :]
+    res = {prec: run(S.Params(n=64, batch=b, precision=prec, dt=0.05, eps=-0.75, eps_per_replica=eps), psi0)
+           for prec in ("fp64", "fp32")}
+    first = 1 if lamellae else 0  # replica 0 of C4' sits on the saddle-node (module docstring)
+    for c, (e64, q64), (e32, q32) in zip(CHECKS, res["fp64"], res["fp32"]):
+        assert np.array_equal(q32, q64), c
+        rel = np.abs(e32 - e64) / np.abs(e64)
+        print(f"C4 lamellae={lamellae} step {c}: energy rel err FP32 vs FP64 max {rel[first:].max():.3e} "
+              f"median {np.median(rel):.3e} (replica 0: {rel[0]:.3e})")
+        assert rel[first:].max() <= etol, (c, rel)

@@ -1,6 +1,7 @@
 """GPU parity of the Neumann-only parts of the path against the FP64 oracle:
-the substrate penalty (cosFFT/comet/cosNoAdvMorph.cpp:67-74, 591-623) and the
-curvature pass (cosFFT/comet/cosNoAdvMorphCurv.cpp:742-965)."""
+the substrate penalty (cosFFT/comet/cosNoAdvMorph.cpp:67-74, 591-623), the
+curvature pass (cosFFT/comet/cosNoAdvMorphCurv.cpp:742-965) and the advected
+step with the sine-transform Stokes velocity (cosFFT/comet/morphSurfK.cpp)."""
 import math
 
 import numpy as np
@@ -8,6 +9,7 @@ import pytest
 
 import smectic3d_b200 as S
 from oracle import sh_oracle as O
+from smectic3d_b200 import _lib as L
 
 pytestmark = pytest.mark.gpu
 
@@ -20,8 +22,8 @@ def rel(a, b):
 
 def oracle_params(p: S.Params) -> O.Params:
     return O.Params(n=p.n, dx=p.dx, dt=p.dt, eps=p.eps, beta=p.beta, gamma=p.gamma, alpha=p.alpha, q0=p.q0,
-                    nonlinearity=p.nonlinearity, scheme=p.scheme, w_mid=p.w_mid, sub_sigma=p.sub_sigma,
-                    sub_z0=p.sub_z0)
+                    eta=p.eta, rho=p.rho, nonlinearity=p.nonlinearity, scheme=p.scheme, w_mid=p.w_mid,
+                    sub_sigma=p.sub_sigma, sub_z0=p.sub_z0)
 
 
 def undulated(n, dx, amp=0.9, phase=0.37):
@@ -104,6 +106,59 @@ def test_curvature_pass_sphere():
         assert abs(kk[i, j] * rr * rr - 1) < 0.03
 
 
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [32, 64])
+def test_spectral_curvature_pass_matches_oracle(n, prec):
+    """curvature = "spectral": the gradient and mixed derivatives are the exact
+    derivatives of the cosine series (sine series through the signed cosine pair
+    on the GPU), against the oracle's scipy DST-III evaluation."""
+    p = S.Params(n=n, boundary="neumann", precision=prec, dt=0.05, eps=-0.7, curvature="spectral")
+    psi0 = undulated(n, p.dx)
+    orc = O.NeumannOracle(psi0, oracle_params(p))
+    orc.run(3)
+    f = O.neumann_curvature_fields(orc)
+    sp = O.neumann_spectral_derivatives(orc.psi, p.dx)
+    zo, vo, ho, ko = O.neumann_curvature_scan(orc.psi, f, p.dx, spectral=sp)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(3)
+        z, vn, hh, kk = s.surface_step()
+    found = zo >= 0
+    assert found.mean() > 0.9
+    same = z == zo
+    assert same.mean() >= (1.0 if prec == "fp64" else 0.99)
+    m = same & found
+    tol = 1e-8 if prec == "fp64" else 2e-3
+    for got, ref in ((vn, vo), (hh, ho), (kk, ko)):
+        scale = max(np.abs(ref[m]).max(), 1e-3)
+        assert np.abs(got[m] - ref[m]).max() <= tol * scale
+
+
+def test_curvature_pass_sphere_spectral_beats_differences():
+    """The sphere known answer (H = 2/r, K = 1/r^2) with both gradient forms: the
+    spectral one is closer at every probed column."""
+    n = 64
+    dx = 2 * math.pi / 32
+    x = np.arange(n) * dx
+    L = n * dx
+    r = np.sqrt((x[:, None, None] - L / 2) ** 2 + (x[None, :, None] - L / 2) ** 2 + (x[None, None, :] + 12.0) ** 2)
+    psi0 = np.cos(r - 12.0 - 0.5 * L - 0.11)
+    err = {}
+    for form in ("difference", "spectral"):
+        p = S.Params(n=n, dx=dx, boundary="neumann", precision="fp64", dt=0.01, eps=-0.7, curvature=form)
+        with S.Solver(p) as s:
+            s.set_psi(psi0)
+            z, vn, hh, kk = s.surface_step()
+        e = []
+        for i, j in ((n // 2, n // 2), (n // 2 + 5, n // 2 - 7), (n // 2 - 10, n // 2 + 3)):
+            assert z[i, j] >= 0
+            rr = r[i, j, z[i, j]]
+            e.append((abs(hh[i, j] * rr / 2 - 1), abs(kk[i, j] * rr * rr - 1)))
+        err[form] = np.array(e)
+    assert (err["spectral"] < err["difference"]).all(), err
+    assert err["spectral"].max() < 5e-3, err
+
+
 @pytest.mark.parametrize("boundary,prec", [("neumann", "fp64"), ("neumann", "fp32"), ("periodic", "fp64")])
 def test_local_amplitude_matches_oracle(boundary, prec):
     """sh_local_amplitude (morphSurfAmp.cpp:1005-1125) on the handle's own psi
@@ -168,3 +223,46 @@ def test_batched_curvature_and_amplitude_match_single_replicas(prec):
         m = z1 >= 0
         for got, ref in ((amp[r], a1), (vn[r][m], v1[m]), (hh[r][m], h1[m]), (kk[r][m], k1[m]), (psi[r], p1r)):
             assert np.allclose(got, ref, rtol=1e-12 if prec == "fp64" else 1e-5, atol=1e-12)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("n", [16, 32, 64, 128])
+def test_advected_neumann_matches_oracle(n, prec):
+    """Neumann step with the Stokes velocity of morphSurfK.cpp (RODFT10/01 through
+    the signed cosine pair on the GPU): psi after 12 steps and the velocity of
+    the final state against the oracle."""
+    p = S.Params(n=n, boundary="neumann", advection=True, precision=prec, dt=0.02, eps=-0.7, eta=0.5)
+    psi0 = undulated(n, p.dx) + S.ic.noise(n, 21, 0.05)
+    orc = O.NeumannOracle(psi0, oracle_params(p), advect=True)
+    orc.run(12)
+    uo, _, _ = orc.velocity(O.dct3d(orc.psi))
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(12)
+        assert rel(s.get_psi(), orc.psi) <= TOL[prec]
+        u = s.velocity()
+    for c in range(3):
+        assert rel(u[c], uo[c]) <= (1e-10 if prec == "fp64" else 1e-4), c
+    assert max(np.abs(x).max() for x in uo) > 1e-4  # the flow is not trivially zero
+
+
+def test_advected_neumann_256_few_steps():
+    """The Neumann advected step at 256^3 (FP32) against the oracle for two steps."""
+    n = 256
+    p = S.Params(n=n, boundary="neumann", advection=True, precision="fp32", dt=0.02, eps=-0.75)
+    psi0 = S.ic.hyperboloid(n, p.dx, amp=1.328, seed=0)
+    orc = O.NeumannOracle(psi0, oracle_params(p), advect=True)
+    orc.run(2)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(2)
+        assert rel(s.get_psi(), orc.psi) <= TOL["fp32"]
+
+
+def test_advected_neumann_refuses_curvature_pass():
+    p = S.Params(n=16, boundary="neumann", advection=True, precision="fp64")
+    with S.Solver(p) as s:
+        s.set_psi(undulated(16, p.dx))
+        with pytest.raises(S.ShError) as e:
+            s.surface_step()
+        assert e.value.code == L.SH_EUNSUPPORTED

@@ -176,6 +176,35 @@ def test_surface_scan_planar_front():
     assert np.isfinite(vn).all()
 
 
+@pytest.mark.parametrize("n", [16, 32])
+def test_surface_scan_vectorised_equals_column_loop(n):
+    """The whole-array scan used for the 256^3 fixtures equals the per-column
+    restatement of surfTrack.cpp:767-806 on doubly curved lamellae."""
+    p = O.Params(n=n, dt=0.02, eps=-0.7)
+    c = np.arange(n) * p.dx
+    lam = n / 2 * p.dx
+    h = 0.83 * p.dx * (np.sin(2 * np.pi * c / lam + 0.3)[:, None, None] + np.cos(2 * np.pi * c / lam + 0.7)[None, :, None])
+    orc = O.PeriodicOracle(1.3 * np.cos(c[None, None, :] - h - 0.37), p, advect=True)
+    orc.run(2)
+    orc.step()
+    f = orc.surface_fields()
+    for a, b in zip(O.surface_scan(orc.psi, *f), O.surface_scan_vec(orc.psi, *f)):
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+def test_dominant_wavenumber_of_single_modes():
+    """A single grid mode puts all its power in its own shell, in both boxes."""
+    n, dx = 32, 2 * math.pi / 8
+    i = np.arange(n)
+    for m in (3, 5):
+        per = np.cos(2 * math.pi * m * i / n)[None, None, :] * np.cos(2 * math.pi * 2 * i / n)[:, None, None]
+        assert math.isclose(O.dominant_wavenumber(np.broadcast_to(per, (n, n, n)), dx),
+                            round(math.hypot(m, 2)) * 2 * math.pi / (n * dx))
+        neu = np.cos(math.pi * m * (i + 0.5) / n)[None, None, :] * np.cos(math.pi * 4 * (i + 0.5) / n)[None, :, None]
+        assert math.isclose(O.dominant_wavenumber_neumann(np.broadcast_to(neu, (n, n, n)), dx),
+                            round(math.hypot(m, 4)) * math.pi / (n * dx))
+
+
 def test_adjoint_matches_finite_differences():
     n = 8
     p = O.Params(n=n, dt=0.05)
@@ -348,6 +377,71 @@ def test_neumann_oracle_against_the_reference_loop_literally():
     orc = O.NeumannOracle(psi0, p)
     orc.run(2)
     assert np.abs(orc.psi - psi).max() <= 1e-13 * np.abs(psi).max()
+
+
+def test_neumann_velocity_against_the_reference_loop_literally():
+    """The Stokes velocity of cosFFT/comet/morphSurfK.cpp (L psi by REDFT01 :686-696,
+    wall-one-sided difference gradients :700-766, stress through RODFT10 :760-770,
+    the projector with the sine wavenumbers :331-348, 624-631, 862-882, RODFT01)
+    with every transform an explicit sum of FFTW's definitions, against the oracle;
+    then one advected step built on it, N = beta psi^3 - gamma psi^5 - u . grad psi."""
+    n, dx, dt, ep, beta, gamma, alpha, q0, rho, eta = 6, 2 * math.pi / 8, 0.05, -0.3, 2.0, 1.0, 1.0, 1.0, 1.0, 1.0
+    p = O.Params(n=n, dx=dx, dt=dt, eps=ep, beta=beta, gamma=gamma, alpha=alpha, q0=q0, rho=rho, eta=eta)
+    psi0 = np.random.default_rng(10).uniform(-0.8, 0.8, size=(n, n, n))
+    kk, nn = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    cfwd = 2.0 * np.cos(math.pi * (2 * nn + 1) * kk / (2 * n))                      # REDFT10[k, n]
+    cinv = (np.where(kk == 0, 1.0, 2.0) * np.cos(math.pi * (2 * nn + 1) * kk / (2 * n))).T  # REDFT01[n, k]
+    sfwd = 2.0 * np.sin(math.pi * (2 * nn + 1) * (kk + 1) / (2 * n))                # RODFT10[k, n]
+    sinv = (np.where(kk == n - 1, 1.0, 2.0) * np.sin(math.pi * (kk + 1) * (2 * nn + 1) / (2 * n))).T  # RODFT01[n, k]
+
+    def t3(m, a):
+        return np.einsum("ai,bj,ck,ijk->abc", m, m, m, a)
+
+    scale = 1.0 / (8.0 * n ** 3)
+    vq = np.array([math.pi * i / (dx * n) for i in range(n)])
+    vs = np.array([math.pi * (i + 1) / (dx * n) for i in range(n)])
+    psi = psi0.copy()
+    psiq = t3(cfwd, psi)
+    op_sh = np.empty((n, n, n))
+    cm1 = np.empty((n, n, n))
+    cm2 = np.empty((3, n, n, n))
+    for i in range(n):
+        for j in range(n):
+            for k in range(n):
+                op_sh[i, j, k] = scale * alpha * (vq[i] ** 2 + vq[j] ** 2 + vq[k] ** 2 - q0 * q0) ** 2
+                mq2 = vs[i] ** 2 + vs[j] ** 2 + vs[k] ** 2
+                cm1[i, j, k] = scale / (rho * eta * mq2)
+                cm2[:, i, j, k] = (vs[i] / mq2, vs[j] / mq2, vs[k] / mq2)
+    psi_sh = t3(cinv, op_sh * psiq)
+    grad = np.empty((3, n, n, n))
+    for ax in range(3):
+        a = np.moveaxis(psi, ax, 0)
+        g = np.empty_like(a)
+        for i in range(n):
+            if 0 < i < n - 1:
+                g[i] = (a[i + 1] - a[i - 1]) / (2 * dx)
+            elif i == 0:
+                g[i] = 2 * (a[1] - a[0]) / (2 * dx)
+            else:
+                g[i] = 2 * (a[i] - a[i - 1]) / (2 * dx)
+        grad[ax] = np.moveaxis(g, 0, ax)
+    sq = np.array([t3(sfwd, psi_sh * grad[c]) for c in range(3)])
+    dot = vs[:, None, None] * sq[0] + vs[None, :, None] * sq[1] + vs[None, None, :] * sq[2]
+    u = np.array([t3(sinv, cm1 * (sq[c] - cm2[c] * dot)) for c in range(3)])
+    orc = O.NeumannOracle(psi0, p, advect=True)
+    uo, go, lo = orc.velocity(O.dct3d(psi0))
+    assert np.abs(np.array(go) - grad).max() <= 1e-13 * np.abs(grad).max()
+    assert np.abs(np.array(uo) - u).max() <= 1e-12 * np.abs(u).max()
+    assert np.abs(u).max() > 1e-6
+    # one advected step: the history N-hat has no advection, the current one has
+    nr = beta * psi ** 3 - gamma * psi ** 5
+    nq_past = t3(cfwd, nr)
+    nq = t3(cfwd, nr - (u * grad).sum(axis=0))
+    c1 = 1.0 + dt / 2 * (ep - op_sh / scale)
+    c2 = 1.0 - dt / 2 * (ep - op_sh / scale)
+    psi1 = t3(cinv, scale * (c1 * psiq + dt / 2 * (3.0 * nq - nq_past)) / c2)
+    orc.step()
+    assert np.abs(orc.psi - psi1).max() <= 1e-12 * np.abs(psi1).max()
 
 
 def test_periodic_oracle_against_the_reference_loop_literally():

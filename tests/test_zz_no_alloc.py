@@ -1,19 +1,21 @@
 """sh_l1_noalloc, the L1 monitor that allocates no device memory, against the
-handle-based monitor behind sh_l1.
+handle-based monitor behind sh_l1 and against the oracle's L1 monitor.
 
 sh_l1_noalloc is for callers that cannot let a library call cudaMalloc:
  - hosts that own all device memory through their own pool;
  - real-time loops that cannot take the implicit synchronisation of an
    allocation.
 This test therefore owns every device buffer it passes. It checks the result
-against the value sh_l1 reports for the same two states, on two calls in a
-row. The second call must not see anything the first one left in the shared
+against the value sh_l1 reports for the same two states and against the
+oracle's monitor evaluated on copies of those states, on two calls in a row.
+The second call must not see anything the first one left in the shared
 scratch array.
 """
 import numpy as np
 import pytest
 
 import smectic3d_b200 as S
+from oracle import sh_oracle as O
 from smectic3d_b200 import _lib as L
 
 pytestmark = pytest.mark.gpu
@@ -48,6 +50,10 @@ def test_l1_noalloc_matches_handle_monitor_twice():
             got = out.cpu().numpy()
             assert np.all(np.isfinite(got))
             assert np.allclose(got, ref, rtol=1e-12, atol=0), (call, got, ref)
+            a_new = new.cpu().numpy().reshape(batch, -1)
+            a_old = old.cpu().numpy().reshape(batch, -1)
+            orc = [O.l1_monitor(a_new[r], a_old[r], p.dt) for r in range(batch)]
+            assert np.allclose(got, orc, rtol=1e-12, atol=0), (call, got, orc)
 
 
 def test_l1_noalloc_rejects_batch_beyond_scratch():
