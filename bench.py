@@ -214,6 +214,14 @@ def timed_steps(solver, k, torch, dist, clocks=None):
     return max_over_ranks(start.elapsed_time(end), torch, dist)
 
 
+def rank_inputs(workload, rank):
+    """Parameters and initial state of one rank: every rank integrates its own
+    domain (replicas only), seeded by its rank."""
+    _, n, batch, _, ick = WORKLOADS[workload]
+    p = params_for(workload)
+    return p, make_ic(ick, n, batch, p.dx, seed=rank)
+
+
 def run_ours(args, rank, world, local_rank, dist):
     import numpy as np
     import torch
@@ -222,8 +230,7 @@ def run_ours(args, rank, world, local_rank, dist):
 
     torch.cuda.set_device(local_rank)
     bnd, n, batch, prec, ick = WORKLOADS[args.workload]
-    p32 = params_for(args.workload)
-    psi0 = make_ic(ick, n, batch, p32.dx, seed=rank)
+    p32, psi0 = rank_inputs(args.workload, rank)
     k, w = args.steps, args.warmup
 
     # ---- device-resident timing of the headline precision -----------------
@@ -250,6 +257,18 @@ def run_ours(args, rank, world, local_rank, dist):
     a64 = s64.get_psi()
     rel_err = float(np.linalg.norm(a32 - a64) / max(np.linalg.norm(a64 if prec == "fp32" else a32), 1e-300))
     s64.close()
+    # FP32 fields with the CNAB2 update in FP64 (the long-run option)
+    u64 = None
+    if prec == "fp32":
+        su = S.Solver(params_for(args.workload, "fp32_u64"))
+        su.set_psi(psi0)
+        su.step(w)
+        su.prepare()
+        msu = timed_steps(su, k, torch, dist)
+        au = su.get_psi()
+        su.close()
+        u64 = {"precision": "fp32_u64", "value": world * k / (msu / 1e3), "ms_per_step": msu / k,
+               "rel_err_vs_fp64": float(np.linalg.norm(au - a64) / np.linalg.norm(a64)), "after_steps": w + k}
 
     # ---- accuracy of the FP32 path after 100 steps (the north-star check),
     # on the workload's IC and on the non-decaying reference-amplitude lamellae
@@ -337,6 +356,7 @@ def run_ours(args, rank, world, local_rank, dist):
                             "rel_err_fp32_vs_fp64": rel_err, "after_steps": w + k,
                             "rel_err_fp32_vs_fp64_after_100_steps": acc100,
                             "energy_rel_err_fp32_vs_fp64_after_100_steps": energy_rel},
+        "fp32_fp64_update": u64,
         "adjoint_forward_ratio": adj["backward_over_forward"] if adj else None,
         "adjoint": adj,
         "other_configs": others,

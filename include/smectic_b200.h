@@ -41,6 +41,8 @@ extern "C" {
 /* arithmetic of fields and transforms */
 #define SH_FP64 0
 #define SH_FP32 1
+#define SH_FP32_UPDATE64 2 /* FP32 fields and transforms; the plain step's CNAB2 multipliers
+                              and update in FP64, which keeps long runs within 1e-6 of FP64 */
 /* gradient and mixed derivatives of the Neumann curvature pass */
 #define SH_CURV_DIFFERENCE 0 /* centred differences, one-sided at the walls (cosNoAdvMorphCurv.cpp:811-940) */
 #define SH_CURV_SPECTRAL 1   /* exact derivatives of the cosine series (sine series through the cosine pair) */
@@ -71,6 +73,8 @@ typedef struct sh_params {
   double sub_z0;
   const double* eps_per_replica; /* NULL, or `batch` values of epsilon       */
   int curvature;     /* Neumann curvature pass: SH_CURV_DIFFERENCE / SH_CURV_SPECTRAL */
+  int replica_block; /* batched plain steps: replicas advanced together, 16 steps at a
+                        time, while their state stays in L2 (0 = all replicas each step) */
 } sh_params;
 
 typedef struct sh_handle sh_handle;

@@ -15,7 +15,7 @@ SH_OK, SH_EINVAL, SH_ENOMEM, SH_ENONFINITE, SH_ETIMEOUT, SH_ECUDA, SH_EUNSUPPORT
 SH_PERIODIC, SH_NEUMANN = 0, 1
 SH_QUINTIC, SH_QUAD_CUBIC = 0, 1
 SH_CNAB2, SH_IMEX_EULER = 0, 1
-SH_FP64, SH_FP32 = 0, 1
+SH_FP64, SH_FP32, SH_FP32_UPDATE64 = 0, 1, 2
 SH_LAYOUT_DENSE, SH_LAYOUT_PADDED = 0, 1
 SH_CURV_DIFFERENCE, SH_CURV_SPECTRAL = 0, 1
 
@@ -36,7 +36,7 @@ class ShParams(C.Structure):
         ("dx", C.c_double), ("dt", C.c_double), ("eps", C.c_double), ("beta", C.c_double),
         ("gamma", C.c_double), ("alpha", C.c_double), ("q0", C.c_double), ("eta", C.c_double),
         ("rho", C.c_double), ("w_mid", C.c_double), ("sub_sigma", C.c_double), ("sub_z0", C.c_double),
-        ("eps_per_replica", C.POINTER(C.c_double)), ("curvature", C.c_int),
+        ("eps_per_replica", C.POINTER(C.c_double)), ("curvature", C.c_int), ("replica_block", C.c_int),
     ]
 
 

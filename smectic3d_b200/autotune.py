@@ -1,12 +1,18 @@
-"""Autotuner for the plane-pass cluster size.
+"""Autotuner for the kernel shapes of a run.
 
 Each built shape offers a few cluster sizes for the plane pass (``variant``):
 - CL = 1 and 2 at 64^3;
 - CL = 1, 2 and 4 at 128^3;
 - CL = 4, 8 and 16 at 256^3.
 
+Batched runs of small grids also choose ``replica_block``: how many replicas
+advance together, 16 steps at a time, while their state stays in the 126 MB L2
+(0: every replica each step).  A block whose CTAs fill the GPU in about one wave
+and whose fields fit L2 wins.
+
 The tuner times a few steps of every built candidate for a given (n, batch,
-boundary, precision, advection) and keeps the fastest. Results are cached in a
+boundary, precision, advection), first the cluster size, then the replica
+block with that cluster size, and keeps the fastest. Results are cached in a
 JSON file keyed by that tuple and by the GPU name, under
 $SMECTIC_B200_CACHE (default ~/.cache/smectic3d_b200/tuned.json).
 """
@@ -21,6 +27,8 @@ from pathlib import Path
 import numpy as np
 
 CANDIDATES = {16: (1,), 32: (1,), 64: (1, 2), 128: (1, 2, 4), 256: (4, 8, 16), 512: (16,)}
+# replicas per L2-resident block, tried for batched plain runs at n <= 128
+BLOCKS = (4, 8, 12, 13, 16, 21, 32)
 
 
 def cache_path() -> Path:
@@ -56,9 +64,11 @@ def _time_variant(p, variant: int, steps: int) -> float:
     return (t1 - t0) / steps
 
 
-def tune(p, steps: int = 20, use_cache: bool = True) -> dict:
-    """Time every built cluster size of ``p``'s shape; returns
-    {"variant": best, "us_per_step": {variant: us}} and caches it."""
+def tune(p, steps: int = 32, use_cache: bool = True) -> dict:
+    """Time every built cluster size of ``p``'s shape, then (batched plain runs)
+    every replica block with the best one; returns {"variant": best,
+    "us_per_step": {variant: us}, "replica_block": b, "us_per_step_by_block":
+    {b: us}} and caches it."""
     gpu = _gpu_name()
     key = _key(p, gpu)
     path = cache_path()
@@ -79,7 +89,17 @@ def tune(p, steps: int = 20, use_cache: bool = True) -> dict:
     if not times:
         raise RuntimeError(f"no plane-pass variant runs for {key}")
     best = min(times, key=times.get)
-    rec = {"variant": best, "us_per_step": {str(k): v for k, v in times.items()}}
+    rec = {"variant": best, "us_per_step": {str(k): v for k, v in times.items()}, "replica_block": 0}
+    blocks = [b for b in BLOCKS if b < p.batch] if p.batch > 1 and p.n <= 128 and not p.advection else []
+    if blocks:
+        bt = {0: times[best]}
+        for b in blocks:
+            try:
+                bt[b] = _time_variant(dataclasses.replace(p, replica_block=b), best, steps) * 1e6
+            except Exception:
+                continue
+        rec["replica_block"] = min(bt, key=bt.get)
+        rec["us_per_step_by_block"] = {str(k): v for k, v in bt.items()}
     cache[key] = rec
     path.parent.mkdir(parents=True, exist_ok=True)
     path.write_text(json.dumps(cache, indent=1, sort_keys=True))
@@ -88,3 +108,9 @@ def tune(p, steps: int = 20, use_cache: bool = True) -> dict:
 
 def best_variant(p) -> int:
     return int(tune(p)["variant"])
+
+
+def best_config(p) -> tuple[int, int]:
+    """(variant, replica_block) of the fastest tuned configuration."""
+    rec = tune(p)
+    return int(rec["variant"]), int(rec.get("replica_block", 0))

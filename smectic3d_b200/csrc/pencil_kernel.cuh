@@ -40,6 +40,7 @@ enum PencilMode : int {
   kPencilAdjInit = 8,  // adjoint: partial of lambda^T -> lambdahat^T, mu partial
   kPencilAdj = 9,      // adjoint step: lambdahat^n = A lambdahat^{n+1} + ghat^n, mu partial, parameter gradients
   kPencilAdjOut = 10,  // adjoint: lambdahat -> its x-inverse partial (for lambda^0 in real space)
+  kPencilStepU64 = 11, // the step of FP32 fields with the CNAB2 multipliers and update in FP64
 };
 // multiplier of kPencilXMul
 enum XMulKind : int {
@@ -84,7 +85,8 @@ struct PencilCfg {
   // FP64 holds twice the registers per value: only its small CTAs (N <= 128) get a budget
   static constexpr int step_warps() { return sizeof(T) == 4 ? SHB_STEP_WARPS : (THREADS <= 64 ? SHB_STEP_WARPS_F64 : 0); }
   static constexpr int min_blocks(int mode) {
-    return (mode == kPencilStep && THREADS <= 256 && step_warps() * 32 / THREADS >= 2) ? step_warps() * 32 / THREADS
+    return ((mode == kPencilStep || mode == kPencilStepU64) && THREADS <= 256 && step_warps() * 32 / THREADS >= 2)
+               ? step_warps() * 32 / THREADS
                                                                                       : 0;
   }
   static_assert(FP % TK == 0, "tile must divide the plane");
@@ -273,7 +275,7 @@ pencil_kernel(PencilArgs<T> a) {
   KahanSum acc;
   const bool want_energy = (a.flags & kFlEnergy) != 0;
 
-  if constexpr (MODE == kPencilStep || MODE == kPencilStepAdv) {
+  if constexpr (MODE == kPencilStep || MODE == kPencilStepU64 || MODE == kPencilStepAdv) {
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
     Ops::forward(v, L, t, tw);
@@ -294,7 +296,7 @@ pencil_kernel(PencilArgs<T> a) {
     // FP64 values of the FP32 update (see below); the scalars stay kernel parameters
     const double epsd = a.pp.eps[rep];
     double qyz0d = 0.0, qyz1d = 0.0;
-    if constexpr (sizeof(T) == 4) {
+    if constexpr (MODE == kPencilStepU64 && sizeof(T) == 4) {
       const double qyd = __ldg(&a.qd[ky]), qz0d = __ldg(&a.qd[kz]);
       qyz0d = qyd * qyd + qz0d * qz0d - a.pp.q0 * a.pp.q0;
       if constexpr (DCT) {
@@ -317,9 +319,9 @@ pencil_kernel(PencilArgs<T> a) {
         // psihat^{n+1} = (psihat + dt Nhat) / (1 - dt aLin),  W' = psihat^{n+1} (IMEX Euler)
         const T d0 = qx2 + qyz0;
         const T a0 = eps - alpha * d0 * d0;
-        if constexpr (sizeof(T) == 4) {
-          // FP32 fields: the per-mode multipliers and the update in FP64 from the
-          // FP64 wavenumbers, one rounding of each stored result.  A multiplier
+        if constexpr (MODE == kPencilStepU64 && sizeof(T) == 4) {
+          // FP32 fields with the per-mode multipliers and the update in FP64 from
+          // the FP64 wavenumbers, one rounding of each stored result.  A multiplier
           // rounded to FP32 repeats the same relative error every step, which
           // drifts a mode's amplitude linearly with the step count.
           const double hd = 0.5 * a.pp.dt;
@@ -717,7 +719,8 @@ pencil_kernel(PencilArgs<T> a) {
       }
   }
 
-  if constexpr (MODE == kPencilStep || MODE == kPencilInit || MODE == kPencilXMul || MODE == kPencilAdjInit ||
+  if constexpr (MODE == kPencilStep || MODE == kPencilStepU64 || MODE == kPencilInit || MODE == kPencilXMul ||
+                MODE == kPencilAdjInit ||
                 MODE == kPencilAdj || MODE == kPencilAdjOut) {
     Ops::inverse_to_line(v, L, t, tw);
     __syncthreads();
@@ -800,7 +803,8 @@ pencil_kernel(PencilArgs<T> a) {
     }
   }
 
-  if (want_energy && (MODE == kPencilStep || MODE == kPencilStepAdv || MODE == kPencilEnergy)) {
+  if (want_energy && (MODE == kPencilStep || MODE == kPencilStepU64 || MODE == kPencilStepAdv ||
+                      MODE == kPencilEnergy)) {
     const double tot = block_sum(acc.s, scratch);
     if (threadIdx.x == 0) a.red[size_t(rep) * gridDim.x + blockIdx.x] = tot;
   }

@@ -179,6 +179,7 @@ int sh_default_params(sh_params* p) {
   p->sub_z0 = 1e-4;
   p->eps_per_replica = nullptr;
   p->curvature = SH_CURV_DIFFERENCE;
+  p->replica_block = 0;
   return SH_OK;
 }
 
@@ -189,7 +190,8 @@ int sh_create(const sh_params* p, sh_handle** out) {
   if (!supported_n(p->n)) return fail(nullptr, SH_EUNSUPPORTED, "n must be one of 16, 32, 64, 128, 256, 512");
   if (p->batch < 1 || p->batch > 65535) return fail(nullptr, SH_EINVAL, "batch must be in [1, 65535]");
   if (p->boundary != SH_PERIODIC && p->boundary != SH_NEUMANN) return fail(nullptr, SH_EINVAL, "bad boundary");
-  if (p->precision != SH_FP64 && p->precision != SH_FP32) return fail(nullptr, SH_EINVAL, "bad precision");
+  if (p->precision != SH_FP64 && p->precision != SH_FP32 && p->precision != SH_FP32_UPDATE64)
+    return fail(nullptr, SH_EINVAL, "bad precision");
   if (p->nonlinearity != SH_QUINTIC && p->nonlinearity != SH_QUAD_CUBIC) return fail(nullptr, SH_EINVAL, "bad nonlinearity");
   if (p->scheme != SH_CNAB2 && p->scheme != SH_IMEX_EULER) return fail(nullptr, SH_EINVAL, "bad scheme");
   if (!(p->dx > 0) || !(p->dt > 0)) return fail(nullptr, SH_EINVAL, "dx and dt must be positive");
@@ -202,9 +204,10 @@ int sh_create(const sh_params* p, sh_handle** out) {
   if (p->variant < 0) return fail(nullptr, SH_EINVAL, "variant must be >= 0");
   if (p->curvature != SH_CURV_DIFFERENCE && p->curvature != SH_CURV_SPECTRAL)
     return fail(nullptr, SH_EINVAL, "bad curvature");
+  if (p->replica_block < 0) return fail(nullptr, SH_EINVAL, "replica_block must be >= 0");
 
   SolverBase* s = nullptr;
-  const bool f32 = p->precision == SH_FP32;
+  const bool f32 = p->precision != SH_FP64;
   if (p->boundary == SH_PERIODIC)
     s = f32 ? make_solver_f32_periodic(p->n, p->variant) : make_solver_f64_periodic(p->n, p->variant);
   else

@@ -142,6 +142,7 @@ struct SolverBase {
   // one that forward sweep ended in
   int adj_nsteps = 0, adj_k = 0;
   long long adj_end = -1;
+  bool adj_last_hist = false;  // the history buffers hold the last segment's states
   virtual int residency(int* out) = 0;
 };
 
@@ -259,6 +260,13 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
+  // the plain step's pencil pass: FP32 fields take their CNAB2 multipliers in
+  // FP64 when the handle asks for it (SH_FP32_UPDATE64)
+  int launch_pencil_step(const PencilArgs<T>& b, int reps = 0) {
+    if (sizeof(T) == 4 && p.precision == SH_FP32_UPDATE64) return launch_pencil<kPencilStepU64>(b, reps);
+    return launch_pencil<kPencilStep>(b, reps);
+  }
+
   // a pencil mode whose shared memory does not fit a CTA is never launched
   template <int MODE>
   int set_pencil_attrs() {
@@ -334,6 +342,7 @@ struct Solver final : SolverBase {
     if ((rc = set_attrs(plane_fn<kPlaneGetPsi>(), PC::SMEM, true))) return rc;
     if ((rc = set_attrs(plane_fn<kPlaneInvReal>(), PC::SMEM, true))) return rc;
     if ((rc = set_pencil_attrs<kPencilStep>())) return rc;
+    if ((rc = set_pencil_attrs<kPencilStepU64>())) return rc;
     if ((rc = set_pencil_attrs<kPencilInit>())) return rc;
     if ((rc = set_pencil_attrs<kPencilEnergy>())) return rc;
     if ((rc = set_pencil_attrs<kPencilStepAdv>())) return rc;
@@ -352,9 +361,9 @@ struct Solver final : SolverBase {
   }
 
   template <int MODE>
-  int launch_plane(const PlaneArgs<T>& a) {
+  int launch_plane(const PlaneArgs<T>& a, int reps = 0) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(N * CL, p.batch, 1);
+    cfg.gridDim = dim3(N * CL, reps > 0 ? reps : p.batch, 1);
     cfg.blockDim = dim3(PC::THREADS, 1, 1);
     cfg.dynamicSmemBytes = PC::SMEM;
     cfg.stream = stream;
@@ -380,9 +389,9 @@ struct Solver final : SolverBase {
   }
 
   template <int MODE>
-  int launch_pencil(const PencilArgs<T>& a) {
+  int launch_pencil(const PencilArgs<T>& a, int reps = 0) {
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(QC::TILES, p.batch, 1);
+    cfg.gridDim = dim3(QC::TILES, reps > 0 ? reps : p.batch, 1);
     cfg.blockDim = dim3(QC::THREADS, 1, 1);
     cfg.dynamicSmemBytes = QC::smem(MODE);
     cfg.stream = stream;
@@ -536,13 +545,51 @@ struct Solver final : SolverBase {
   bool graph_eligible() const {
     return use_graphs && !prof_ms && !hist_spec && !p.energy_trace && p.l1_interval == 0;
   }
+  // Replica blocks (batched plain steps, replica_block = g > 0): the graph
+  // advances replicas [0, g) by kGraphChunk steps, then [g, 2g), and so on, so
+  // a block's W, P and N-hat (3 fields per replica) stay in L2 across its steps
+  // and the passes read and write L2 instead of HBM
+  bool blocked() const {
+    return p.replica_block > 0 && p.replica_block < p.batch && !p.advection && kwall == 0;
+  }
+  // n plain steps of replicas [r0, r0 + g) only: every per-replica pointer of the
+  // two passes is offset to the block (no diagnostics, no history)
+  int step_window(int r0, int g, int n) {
+    int rc;
+    const size_t off = size_t(r0) * N * FP;
+    for (int s = 0; s < n; ++s) {
+      PencilArgs<T> b = pencil_args();
+      b.src = Nt + off;
+      b.w = W + off;
+      b.dst = P + off;
+      b.pp.eps = d_eps + r0;
+      if ((rc = launch_pencil_step(b, g))) return rc;
+      PlaneArgs<T> a = plane_args_step();
+      a.src = P + off;
+      a.dst = Nt + off;
+      a.pp.eps = d_eps + r0;
+      if ((rc = launch_plane<kPlaneStep>(a, g))) return rc;
+    }
+    return SH_OK;
+  }
+
   // capture kGraphChunk steps once (nothing runs; the steps counter is restored)
   int build_graph() override {
     if (graph_exec || !graph_eligible()) return SH_OK;
     cudaGraph_t g;
     const long long s0 = steps, l0 = launches;
     SHB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    const int rc = step_direct(kGraphChunk);
+    int rc = SH_OK;
+    if (blocked()) {
+      for (int r0 = 0; r0 < p.batch && !rc; r0 += p.replica_block) {
+        const int gsz = r0 + p.replica_block <= p.batch ? p.replica_block : p.batch - r0;
+        rc = step_window(r0, gsz, kGraphChunk);
+      }
+      steps += kGraphChunk;
+      hist_pos += kGraphChunk;
+    } else {
+      rc = step_direct(kGraphChunk);
+    }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
     steps = s0;
     hist_pos -= kGraphChunk;
@@ -610,7 +657,7 @@ struct Solver final : SolverBase {
           if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
           if ((rc = substrate_lperp())) return rc;
         } else {
-          if ((rc = launch_pencil<kPencilStep>(b))) return rc;
+          if ((rc = launch_pencil_step(b))) return rc;
           if (prof_ms) SHB_CUDA(cudaEventRecord(prof_ev[1], stream));
         }
         PlaneArgs<T> a = plane_args_step();
@@ -921,6 +968,16 @@ struct Solver final : SolverBase {
       ADJ_CUDA(dev_malloc(&bf.ck, size_t(nseg) * 3 * fe * sizeof(cplx<T>)));
       bf.nseg = nseg;
     }
+    if (bf.k < K) {
+      cudaFree(bf.hs);
+      cudaFree(bf.hr);
+      bf.hs = nullptr;
+      bf.hr = nullptr;
+      bf.k = 0;
+      ADJ_CUDA(dev_malloc(&bf.hs, size_t(K + 1) * fe * sizeof(cplx<T>)));
+      ADJ_CUDA(dev_malloc(&bf.hr, size_t(K + 1) * nr * sizeof(T)));
+      bf.k = K;
+    }
     const size_t fb = fe * sizeof(cplx<T>);
     ADJ_CUDA(cudaMemcpyAsync(d_psi, psi0, nr * sizeof(double), cudaMemcpyHostToDevice, stream));
     ADJ_RC(init_from_psi());
@@ -930,13 +987,34 @@ struct Solver final : SolverBase {
       ADJ_CUDA(cudaMemcpyAsync(c + fe, P, fb, cudaMemcpyDeviceToDevice, stream));
       ADJ_CUDA(cudaMemcpyAsync(c + 2 * fe, Nt, fb, cudaMemcpyDeviceToDevice, stream));
       const int s1 = (sg + 1) * K < nsteps ? (sg + 1) * K : nsteps;
-      ADJ_RC(step_async(s1 - sg * K));
+      if (sg == nseg - 1) {
+        // the last segment keeps its states (psihat^n pencil-major, psi^n real) as
+        // the reverse sweep needs them, so the backward does not recompute it
+        PencilArgs<T> b = pencil_args();
+        b.src = P;
+        b.spec_out = bf.hs;
+        ADJ_RC(launch_pencil<kPencilSpec>(b));
+        PlaneArgs<T> a = plane_args();
+        a.src = P;
+        a.real_out = bf.hr;
+        ADJ_RC(launch_plane<kPlaneInvReal>(a));
+        hist_spec = bf.hs;
+        hist_real = bf.hr;
+        hist_pos = 0;
+        rc = step_async(s1 - sg * K);
+        hist_spec = nullptr;
+        hist_real = nullptr;
+        ADJ_RC(rc);
+      } else {
+        ADJ_RC(step_async(s1 - sg * K));
+      }
     }
     restore();
     psi0_valid = false;
     adj_nsteps = nsteps;
     adj_k = K;
     adj_end = steps;
+    adj_last_hist = true;
     return SH_OK;
   }
 
@@ -1009,26 +1087,29 @@ struct Solver final : SolverBase {
       for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * K;
         const int s1 = (sg + 1) * K < nsteps ? (sg + 1) * K : nsteps;
-        const cplx<T>* c = bf.ck + size_t(sg) * 3 * fe;
-        ADJ_CUDA(cudaMemcpyAsync(W, c, fb, cudaMemcpyDeviceToDevice, stream));
-        ADJ_CUDA(cudaMemcpyAsync(P, c + fe, fb, cudaMemcpyDeviceToDevice, stream));
-        ADJ_CUDA(cudaMemcpyAsync(Nt, c + 2 * fe, fb, cudaMemcpyDeviceToDevice, stream));
-        {  // psihat^{s0} and psi^{s0} of the segment's first state
-          PencilArgs<T> b = pencil_args();
-          b.src = P;
-          b.spec_out = bf.hs;
-          ADJ_RC(launch_pencil<kPencilSpec>(b));
-          PlaneArgs<T> a = plane_args();
-          a.src = P;
-          a.real_out = bf.hr;
-          ADJ_RC(launch_plane<kPlaneInvReal>(a));
+        if (!(sg == nseg - 1 && adj_last_hist)) {  // the forward sweep kept the last segment's states
+          adj_last_hist = false;                    // this recompute overwrites them
+          const cplx<T>* c = bf.ck + size_t(sg) * 3 * fe;
+          ADJ_CUDA(cudaMemcpyAsync(W, c, fb, cudaMemcpyDeviceToDevice, stream));
+          ADJ_CUDA(cudaMemcpyAsync(P, c + fe, fb, cudaMemcpyDeviceToDevice, stream));
+          ADJ_CUDA(cudaMemcpyAsync(Nt, c + 2 * fe, fb, cudaMemcpyDeviceToDevice, stream));
+          {  // psihat^{s0} and psi^{s0} of the segment's first state
+            PencilArgs<T> b = pencil_args();
+            b.src = P;
+            b.spec_out = bf.hs;
+            ADJ_RC(launch_pencil<kPencilSpec>(b));
+            PlaneArgs<T> a = plane_args();
+            a.src = P;
+            a.real_out = bf.hr;
+            ADJ_RC(launch_plane<kPlaneInvReal>(a));
+          }
+          hist_spec = bf.hs;
+          hist_real = bf.hr;
+          hist_pos = 0;
+          ADJ_RC(step_async(s1 - s0));
+          hist_spec = nullptr;
+          hist_real = nullptr;
         }
-        hist_spec = bf.hs;
-        hist_real = bf.hr;
-        hist_pos = 0;
-        ADJ_RC(step_async(s1 - s0));
-        hist_spec = nullptr;
-        hist_real = nullptr;
         for (int n = s1 - 1; n >= s0; --n) {
           const int j = n - s0;
           PlaneArgs<T> a = plane_args();

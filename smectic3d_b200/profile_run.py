@@ -27,11 +27,14 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=4)
     ap.add_argument("--variant", type=int, default=0)
     ap.add_argument("--advection", action="store_true")
+    ap.add_argument("--replica-block", type=int, default=0,
+                    help="batched runs: replicas per L2-resident block (0 = all replicas each step)")
     ap.add_argument("--adjoint", type=int, default=0, metavar="T",
                     help="instead of plain steps, run sh_adjoint over T steps (checkpoints every 50)")
     args = ap.parse_args(argv)
     p = Params(n=args.n, batch=args.batch, boundary=args.boundary, precision=args.precision, variant=args.variant,
-               advection=args.advection)
+               advection=args.advection, replica_block=args.replica_block,
+               eps_per_replica=tuple(np.linspace(-0.9, -0.5, args.batch)) if args.batch > 1 else None)
     with Solver(p) as s:
         psi = np.stack([noise(args.n, r) for r in range(args.batch)]) if args.batch > 1 else noise(args.n, 0)
         s.set_psi(psi)

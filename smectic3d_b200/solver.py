@@ -25,7 +25,7 @@ class Params:
     advection: bool = False
     nonlinearity: str = "quintic"    # beta psi^3 - gamma psi^5 (reference) | "quad_cubic"
     scheme: str = "cnab2"            # reference CN + AB2 | "imex_euler"
-    precision: str = "fp64"          # "fp64" | "fp32"
+    precision: str = "fp64"          # "fp64" | "fp32" | "fp32_u64" (FP32 fields, FP64 CNAB2 update)
     l1_interval: int = 0             # 100 in the reference (periodicFFT/pf3d.cpp:489)
     energy_trace: bool = False
     dx: float = 2.0 * math.pi / 8.0
@@ -43,6 +43,7 @@ class Params:
     eps_per_replica: tuple | None = None
     variant: int = 0                 # plane-pass cluster size (0 = default, -1 = autotune)
     curvature: str = "difference"    # Neumann curvature pass: "difference" (reference) | "spectral"
+    replica_block: int = 0           # batched plain steps: replicas per L2-resident block (0 = off)
 
     @staticmethod
     def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":
@@ -56,11 +57,12 @@ class Params:
         p.advection = int(bool(self.advection))
         p.nonlinearity = {"quintic": L.SH_QUINTIC, "quad_cubic": L.SH_QUAD_CUBIC}[self.nonlinearity]
         p.scheme = {"cnab2": L.SH_CNAB2, "imex_euler": L.SH_IMEX_EULER}[self.scheme]
-        p.precision = {"fp64": L.SH_FP64, "fp32": L.SH_FP32}[self.precision]
+        p.precision = {"fp64": L.SH_FP64, "fp32": L.SH_FP32, "fp32_u64": L.SH_FP32_UPDATE64}[self.precision]
         p.l1_interval = self.l1_interval
         p.energy_trace = int(bool(self.energy_trace))
         p.variant = int(self.variant)
         p.curvature = {"difference": L.SH_CURV_DIFFERENCE, "spectral": L.SH_CURV_SPECTRAL}[self.curvature]
+        p.replica_block = int(self.replica_block)
         for k in ("dx", "dt", "eps", "beta", "gamma", "alpha", "q0", "eta", "rho", "w_mid", "sub_sigma", "sub_z0"):
             setattr(p, k, float(getattr(self, k)))
         keep = None
@@ -76,8 +78,9 @@ class Solver:
     def __init__(self, params: Params):
         self.lib = L.load()
         if params.variant < 0:
-            from .autotune import best_variant
-            params = dataclasses.replace(params, variant=best_variant(dataclasses.replace(params, variant=0)))
+            from .autotune import best_config
+            v, blk = best_config(dataclasses.replace(params, variant=0))
+            params = dataclasses.replace(params, variant=v, replica_block=blk)
         self.params = params
         cp, keep = params.to_c()
         h = C.c_void_p()

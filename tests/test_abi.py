@@ -40,8 +40,9 @@ def test_params_struct_layout_matches_header():
 #include <stddef.h>
 #include "smectic_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(sh_params), offsetof(sh_params, dx), offsetof(sh_params, w_mid),
-         offsetof(sh_params, sub_z0), offsetof(sh_params, eps_per_replica), offsetof(sh_params, curvature));
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(sh_params), offsetof(sh_params, dx), offsetof(sh_params, w_mid),
+         offsetof(sh_params, sub_z0), offsetof(sh_params, eps_per_replica), offsetof(sh_params, curvature),
+         offsetof(sh_params, replica_block));
   return 0;
 }
 """
@@ -54,7 +55,7 @@ int main(void) {
     got = [int(v) for v in out]
     P = L.ShParams
     assert got == [C.sizeof(P), P.dx.offset, P.w_mid.offset, P.sub_z0.offset, P.eps_per_replica.offset,
-                   P.curvature.offset]
+                   P.curvature.offset, P.replica_block.offset]
 
 
 def test_default_params(lib):

@@ -64,3 +64,25 @@ def test_keys_separate_shapes(fake, monkeypatch):
     autotune.tune(S.Params(n=64, precision="fp32", batch=8), steps=3)
     autotune.tune(S.Params(n=64, precision="fp32", batch=8, boundary="neumann"), steps=3)
     assert len(json.loads(cache.read_text())) == 2
+
+
+def test_replica_block_is_tuned_for_batched_runs(fake, monkeypatch):
+    """Batched plain runs then try replica blocks below the batch with the best
+    cluster size; the fastest (or no blocking) is kept."""
+    cache, calls, _ = fake
+    seen = []
+
+    def _time_variant(p, v, steps):
+        seen.append((v, p.replica_block))
+        base = {1: 100.0, 2: 120.0}[v]
+        return (base - (40.0 if p.replica_block == 13 else 0.0)) * 1e-6
+    monkeypatch.setattr(autotune, "_time_variant", _time_variant)
+    rec = autotune.tune(S.Params(n=64, precision="fp32", batch=64), steps=3)
+    assert rec["variant"] == 1 and rec["replica_block"] == 13
+    assert seen[:2] == [(1, 0), (2, 0)]
+    assert {b for v, b in seen[2:]} == {4, 8, 12, 13, 16, 21, 32} and all(v == 1 for v, _ in seen[2:])
+    assert autotune.best_config(S.Params(n=64, precision="fp32", batch=64)) == (1, 13)
+    # single domains and advected runs are not blocked
+    seen.clear()
+    rec = autotune.tune(S.Params(n=64, precision="fp32", batch=1), steps=3)
+    assert rec["replica_block"] == 0 and all(b == 0 for _, b in seen)

@@ -149,13 +149,29 @@ def test_linear_growth_factor_full_size(n, prec, boundary):
         assert rel(s.get_psi(), g ** 3 * psi0) <= (1e-12 if prec == "fp64" else 1e-6)
 
 
-def test_fp64_512_advection_reports_unsupported():
-    """512^3 in FP64 runs the plain and Neumann steps (the plane pass exchanges
-    by direct stores there); the Stokes pencil pass needs more shared memory
-    per CTA than there is, so advection at that size is refused."""
-    with pytest.raises(S.ShError) as e:
-        S.Solver(S.Params(n=512, precision="fp64", advection=True))
-    assert e.value.code == L.SH_EUNSUPPORTED
+@pytest.mark.parametrize("n,prec", [(256, "fp32"), (512, "fp64")])
+def test_advected_single_mode_is_the_plain_growth(n, prec):
+    """Known answer for the advected step at full size (512^3 FP64 runs its plane
+    passes with direct exchanges): for psi = A cos(q z) the stress
+    S = (L psi) grad psi = -(1/2) opSH q A^2 sin(2 q z) e_z is a gradient, the
+    projector removes it, u = 0, and with beta = gamma = 0 every step multiplies
+    the mode by (1 + dt a/2)/(1 - dt a/2)."""
+    p = S.Params(n=n, precision=prec, dt=0.1, eps=0.1, beta=0.0, gamma=0.0, advection=True)
+    m = n // 8 + 1
+    q = 2 * math.pi * m / (n * p.dx)
+    psi0 = 1e-3 * np.broadcast_to(np.cos(2 * math.pi * m * np.arange(n) / n)[None, None, :], (n, n, n)).copy()
+    a = p.eps - (q * q - 1.0) ** 2
+    g = (1 + p.dt * a / 2) / (1 - p.dt * a / 2)
+    with S.Solver(p) as s:
+        s.set_psi(psi0)
+        s.step(3)
+        assert rel(s.get_psi(), g ** 3 * psi0) <= (1e-12 if prec == "fp64" else 1e-6)
+        u = s.velocity()
+    # the velocity the projector removed, |S| / (rho eta q^2) with S = (1/2) opSH q A^2,
+    # is left at the level of the transforms' rounding (FP32: the rounding noise of
+    # L psi grows with opSH at large |k|)
+    removed = 0.5 * (q * q - 1.0) ** 2 * q * 1e-6 / (q * q)
+    assert max(np.abs(c).max() for c in u) <= (1e-10 if prec == "fp64" else 1e-2) * removed
 
 
 @pytest.mark.parametrize("boundary", ["periodic", "neumann"])
@@ -240,6 +256,29 @@ def test_batched_replicas_are_independent(prec):
         assert rel(allpsi[r], orc.psi) <= TOL[prec]
         eo = O.energy_spectral_periodic(orc.psi, oracle_params(S.Params(n=n, eps=eps[r])))
         assert abs(eb[r] - eo) <= ETOL[prec] * abs(eo)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "fp32"])
+@pytest.mark.parametrize("boundary", ["periodic", "neumann"])
+def test_replica_blocks_are_bit_exact(boundary, prec):
+    """replica_block: blocks of replicas take 16 steps at a time while their state
+    stays in L2; every replica's result is bit for bit the unblocked one, and
+    replica 0 matches the oracle."""
+    n, b = 64, 11
+    eps = np.linspace(-0.9, -0.5, b)
+    psi0 = S.ic.noise_batch(n, range(b), 0.3) + 1.3 * np.cos(np.arange(n) * 2 * math.pi / 8)[None, None, None, :]
+    out = {}
+    for blk in (0, 4):
+        p = S.Params(n=n, batch=b, boundary=boundary, precision=prec, eps_per_replica=tuple(eps), replica_block=blk)
+        with S.Solver(p) as s:
+            s.set_psi(psi0)
+            s.step(40)  # two replayed 16-step blocks and 8 direct steps
+            out[blk] = s.get_psi()
+    assert np.array_equal(out[0], out[4])
+    q = S.Params(n=n, boundary=boundary, eps=eps[0])
+    orc = (O.PeriodicOracle if boundary == "periodic" else O.NeumannOracle)(psi0[0], oracle_params(q))
+    orc.run(40)
+    assert rel(out[4][0], orc.psi) <= TOL[prec]
 
 
 @pytest.mark.parametrize("boundary", ["periodic", "neumann"])
