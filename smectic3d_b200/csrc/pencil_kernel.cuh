@@ -276,6 +276,12 @@ pencil_kernel(PencilArgs<T> a) {
   const bool want_energy = (a.flags & kFlEnergy) != 0;
 
   if constexpr (MODE == kPencilStep || MODE == kPencilStepU64 || MODE == kPencilStepAdv) {
+    // this CTA's rows of W (TK x N complex, contiguous) are read after the forward
+    // transform: start bringing them into L2 now
+    if (threadIdx.x == 0)
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.w + (size_t(rep) * FP + f0) * N),
+                   "r"(uint32_t(size_t(TK) * N * sizeof(cplx<T>)))
+                   : "memory");
     Ops::load_tile(buf, a.src + plane_base, f0);
     __syncthreads();
     Ops::forward(v, L, t, tw);

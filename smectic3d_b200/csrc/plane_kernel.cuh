@@ -245,10 +245,18 @@ struct Xchg {
   bool armed;  // an arrive is outstanding (the next cluster_wait completes it)
 };
 
+// The arrives of the bulk protocol carry no memory ordering (.relaxed): what a
+// peer waits for is either the completion of copies this CTA has already
+// observed on its mbarrier (the copy engine has finished reading the peer's send
+// blocks), or the end of this CTA's reads of its receive blocks, whose values
+// are already consumed; the data itself is ordered by the mbarrier (complete_tx,
+// then try_wait with acquire) and by the async-proxy fence before each copy.  A
+// release arrive would add a memory barrier to every phase.  The first arrive
+// follows the fence.mbarrier_init.release.cluster of the mbarrier set-up.
 template <typename T, int CL>
 __device__ __forceinline__ void xchg_arrive(Xchg<T>& x) {
   if constexpr (CL > 1) {
-    cluster_arrive<CL>();
+    asm volatile("barrier.cluster.arrive.relaxed.aligned;" ::: "memory");
     x.armed = true;
   }
 }

@@ -30,7 +30,7 @@ struct Opts {
   long long max_steps = -1;
   double dt = 0.001, eps = -0.7, beta = 2.0, gamma = 1.0, alpha = 1.0, q0 = 1.0, eta = 1.0, rho = 1.0, w_mid = 0.0;
   double l1_limit = 1e-6;
-  std::string boundary = "periodic", precision = "fp64", ic = "lamellae", out = ".";
+  std::string boundary = "periodic", precision = "fp64", ic = "lamellae", out = ".", curvature = "difference";
   bool advection = false;
 };
 
@@ -38,7 +38,8 @@ void usage() {
   std::puts(
       "usage: smectic_run [--n N] [--nw Nw] [--dt dt] [--eps e] [--beta b] [--gamma g] [--alpha a] [--q0 q]\n"
       "                   [--eta h] [--rho r] [--w-mid w] [--boundary periodic|neumann] [--advection]\n"
-      "                   [--precision fp64|fp32] [--ic lamellae|torus|hyperboloid|load:FILE]\n"
+      "                   [--precision fp64|fp32|fp32_u64] [--ic lamellae|torus|hyperboloid|load:FILE]\n"
+      "                   [--curvature difference|spectral]\n"
       "                   [--l1-limit x] [--l1-every k] [--save-every m] [--max-steps s] [--out DIR]\n"
       "                   [--sub-sigma s] [--sub-z0 z0] [--surface-every m] [--amp-nw Nw]\n"
       "  --surface-every m  every m-th L1 evaluation, end the block with the surface pass and append\n"
@@ -87,6 +88,7 @@ bool parse(int argc, char** argv, Opts& o) {
     else if (a == "--surface-every") o.surface_every = std::atoi(need("--surface-every"));
     else if (a == "--amp-nw") o.amp_nw = std::atoi(need("--amp-nw"));
     else if (a == "--alternate") o.alternate = true;
+    else if (a == "--curvature") o.curvature = need("--curvature");
     else {
       std::fprintf(stderr, "unknown option %s\n", a.c_str());
       usage();
@@ -175,7 +177,8 @@ int main(int argc, char** argv) {
   p.w_mid = o.w_mid;
   p.boundary = o.boundary == "neumann" ? SH_NEUMANN : SH_PERIODIC;
   p.advection = o.advection ? 1 : 0;
-  p.precision = o.precision == "fp32" ? SH_FP32 : SH_FP64;
+  p.precision = o.precision == "fp32" ? SH_FP32 : (o.precision == "fp32_u64" ? SH_FP32_UPDATE64 : SH_FP64);
+  p.curvature = o.curvature == "spectral" ? SH_CURV_SPECTRAL : SH_CURV_DIFFERENCE;
   p.l1_interval = o.l1_every;
   p.sub_sigma = o.sub_sigma;
   p.sub_z0 = o.sub_z0;
