@@ -76,6 +76,35 @@ __device__ __forceinline__ cplx<T> cscale(cplx<T> a, T s) { return mk<T>(a.x * s
 template <typename T>
 __device__ __forceinline__ cplx<T> conjg(cplx<T> a) { return mk<T>(a.x, -a.y); }
 
+// ---------------------------------------------------------------------------
+// Global tile traffic.  The passes move tiles between HBM and shared memory with
+// every thread owning E elements.  In FP32 a thread owns consecutive element
+// pairs, so that each pair of complex floats moves as one 16-byte access (the
+// tiles start on even elements of 16-byte aligned buffers); FP64 complex values
+// are 16 bytes already.
+// ---------------------------------------------------------------------------
+#ifndef SHB_PAIR_IO
+#define SHB_PAIR_IO 1
+#endif
+template <typename T>
+__host__ __device__ constexpr bool pair_io() { return SHB_PAIR_IO && sizeof(T) == 4; }
+// element index of register slot e (0 <= e < E) of thread tid of nthr
+template <bool PAIRS>
+__device__ __forceinline__ int tile_elem(int tid, int nthr, int e) {
+  if constexpr (PAIRS) return 2 * (tid + nthr * (e >> 1)) + (e & 1);
+  else return tid + nthr * e;
+}
+__device__ __forceinline__ void ld_pair(const float2* p, float2& a, float2& b) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  a = make_float2(v.x, v.y);
+  b = make_float2(v.z, v.w);
+}
+__device__ __forceinline__ void st_pair(float2* p, float2 a, float2 b) {
+  *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ void ld_pair(const double2*, double2&, double2&) {}
+__device__ __forceinline__ void st_pair(double2*, double2, double2) {}
+
 // padded index inside a shared-memory line
 __host__ __device__ constexpr int pad(int i) { return i + (i >> 4); }
 // line stride in elements (odd spacing between lines of a tile)

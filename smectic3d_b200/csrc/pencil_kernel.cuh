@@ -123,25 +123,33 @@ struct PencilOps {
   using Cfg = PencilCfg<T, N, DCT>;
   static constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
 
+  // the TK lines of a tile are consecutive in memory (f0 and TK even: 16-byte pairs)
+  static constexpr bool PAIRS = pair_io<T>() && TK % 2 == 0;
+  static __device__ __forceinline__ int elem(int e) { return tile_elem<PAIRS>(threadIdx.x, Cfg::THREADS, e); }
+
   // TK * N == THREADS * E: all E loads of a thread are issued before its stores
   static __device__ __forceinline__ void load_tile(cplx<T>* buf, const cplx<T>* __restrict__ src, int f0) {
     cplx<T> tmp[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int idx = threadIdx.x + Cfg::THREADS * e;
-      tmp[e] = src[size_t(idx / TK) * FP + f0 + idx % TK];
+    for (int e = 0; e < E; e += PAIRS ? 2 : 1) {
+      const int idx = elem(e);
+      const cplx<T>* p = &src[size_t(idx / TK) * FP + f0 + idx % TK];
+      if constexpr (PAIRS) ld_pair(p, tmp[e], tmp[e + 1]);
+      else tmp[e] = *p;
     }
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const int idx = threadIdx.x + Cfg::THREADS * e;
+      const int idx = elem(e);
       buf[(idx % TK) * LS + pad(idx / TK)] = tmp[e];
     }
   }
   static __device__ __forceinline__ void store_tile(const cplx<T>* buf, cplx<T>* __restrict__ dst, int f0) {
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int idx = threadIdx.x + Cfg::THREADS * e;
-      dst[size_t(idx / TK) * FP + f0 + idx % TK] = buf[(idx % TK) * LS + pad(idx / TK)];
+    for (int e = 0; e < E; e += PAIRS ? 2 : 1) {
+      const int idx = elem(e);
+      cplx<T>* p = &dst[size_t(idx / TK) * FP + f0 + idx % TK];
+      if constexpr (PAIRS) st_pair(p, buf[(idx % TK) * LS + pad(idx / TK)], buf[(idx % TK + 1) * LS + pad(idx / TK)]);
+      else *p = buf[(idx % TK) * LS + pad(idx / TK)];
     }
   }
 

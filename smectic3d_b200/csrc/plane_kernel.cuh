@@ -346,6 +346,10 @@ struct PlaneOps {
   using Cfg = PlaneCfg<T, N, CL, DCT>;
   static constexpr int E = Cfg::E, G = Cfg::G, NC = Cfg::NC, LS = Cfg::LS, ROWS = Cfg::ROWS;
   static constexpr int THREADS = Cfg::THREADS;
+  // a CTA's NC columns of a plane row are consecutive in memory (c0 and NC even:
+  // 16-byte pairs)
+  static constexpr bool PAIRS = pair_io<T>() && NC % 2 == 0;
+  static __device__ __forceinline__ int elem(int e) { return tile_elem<PAIRS>(threadIdx.x, THREADS, e); }
 
   // ---- column phase, inverse direction ---------------------------------
   // multiply a periodic spectral value at (ky, kz) by i q_y, i q_z or -q_y^2
@@ -382,24 +386,33 @@ struct PlaneOps {
     // NC * N == THREADS * E: every thread issues its E loads before any store
     cplx<T> tmp[E];
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int idx = threadIdx.x + THREADS * e;
+    for (int e = 0; e < E; e += PAIRS ? 2 : 1) {
+      const int idx = elem(e);
       const int row = mult == kMulSinDy ? (N - idx / NC) & (N - 1) : idx / NC;  // reversed rows for d/dy
-      tmp[e] = plane[row * (N / 2) + c0 + idx % NC];
+      const cplx<T>* p = &plane[row * (N / 2) + c0 + idx % NC];
+      if constexpr (PAIRS) ld_pair(p, tmp[e], tmp[e + 1]);
+      else tmp[e] = *p;
     }
     if (mult != kMulNone) {
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + THREADS * e;
+        const int idx = elem(e);
         tmp[e] = apply_mult(tmp[e], mult, q, idx / NC, c0 + idx % NC);
       }
     }
     if (plane2) {
+      cplx<T> u[E];
+#pragma unroll
+      for (int e = 0; e < E; e += PAIRS ? 2 : 1) {
+        const int idx = elem(e);
+        const cplx<T>* p = &plane2[(idx / NC) * (N / 2) + c0 + idx % NC];
+        if constexpr (PAIRS) ld_pair(p, u[e], u[e + 1]);
+        else u[e] = *p;
+      }
 #pragma unroll
       for (int e = 0; e < E; ++e) {
-        const int idx = threadIdx.x + THREADS * e;
-        const cplx<T> u = apply_mult(plane2[(idx / NC) * (N / 2) + c0 + idx % NC], mult2, q, idx / NC, c0 + idx % NC);
-        tmp[e] = cadd<T>(tmp[e], u);
+        const int idx = elem(e);
+        tmp[e] = cadd<T>(tmp[e], apply_mult(u[e], mult2, q, idx / NC, c0 + idx % NC));
       }
     }
     constexpr int KPT = (N + THREADS - 1) / THREADS;  // ky per thread for the kz=0 / N/2 columns
@@ -418,7 +431,7 @@ struct PlaneOps {
     }
 #pragma unroll
     for (int e = 0; e < E; ++e) {
-      const int idx = threadIdx.x + THREADS * e;
+      const int idx = elem(e);
       buf[(idx % NC) * LS + pad(idx / NC)] = tmp[e];
     }
     if constexpr (!DCT) {
@@ -789,9 +802,11 @@ struct PlaneOps {
     }
     const int c0 = rank * NC;
 #pragma unroll
-    for (int e = 0; e < E; ++e) {
-      const int idx = threadIdx.x + THREADS * e;
-      plane[(idx / NC) * (N / 2) + c0 + idx % NC] = cb[(idx % NC) * LS + pad(idx / NC)];
+    for (int e = 0; e < E; e += PAIRS ? 2 : 1) {
+      const int idx = elem(e);
+      cplx<T>* p = &plane[(idx / NC) * (N / 2) + c0 + idx % NC];
+      if constexpr (PAIRS) st_pair(p, cb[(idx % NC) * LS + pad(idx / NC)], cb[(idx % NC + 1) * LS + pad(idx / NC)]);
+      else *p = cb[(idx % NC) * LS + pad(idx / NC)];
     }
     if constexpr (!DCT) {
       if (rank == 0) {
