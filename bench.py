@@ -338,9 +338,9 @@ def run_ours(args, rank, world, local_rank, dist):
         "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": k, "warmup": w,
         "ms_per_step": ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if prec == "fp32" else "f64", "data": "synthetic",
-        "config": {"workload": workload_label(args.workload),
-                   "precision": prec, "parallelism": f"replicas x{world}",
-                   "l2": f"inputs larger than L2: working set {3 * field_mb:.0f} MB > 126 MB, no flush"},
+        "config": bench_config(args),
+        "precision": prec, "parallelism": f"replicas x{world}",
+        "l2": f"inputs larger than L2: working set {3 * field_mb:.0f} MB > 126 MB, no flush",
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": ab[dom], "avg_launch_ms": per[dom],
@@ -597,10 +597,15 @@ def run_reference(args, rank, budget_s=180.0):
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": "steps/s", "n_gpus": args.gpus, "steps": k,
             "warmup": w, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic",
-            "config": {"workload": workload_label(args.workload), "precision": "fp64 (CPU oracle port)",
-                       "parallelism": f"{os.cpu_count()} host threads"},
+            "config": bench_config(args), "precision": "fp64 (CPU oracle port)",
+            "parallelism": f"{os.cpu_count()} host threads",
             "cpu_baseline": cb, "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
+
+
+def bench_config(args) -> dict:
+    """The workload both arms measure (the same dict in the GPU line and the reference line)."""
+    return {"workload": workload_label(args.workload)}
 
 
 def main():
