@@ -270,7 +270,7 @@ def run_ours(args, rank, world, local_rank, dist):
         u64 = {"precision": "fp32_u64", "value": world * k / (msu / 1e3), "ms_per_step": msu / k,
                "rel_err_vs_fp64": float(np.linalg.norm(au - a64) / np.linalg.norm(a64)), "after_steps": w + k}
 
-    # ---- accuracy of the FP32 path after 100 steps (the north-star check),
+    # ---- accuracy of the FP32 path after 100 steps (the 1e-5 accuracy bound),
     # on the workload's IC and on the non-decaying reference-amplitude lamellae
     acc100, energy_rel = {}, {}
     for label, ic0 in (("workload_ic", psi0),
