@@ -225,6 +225,17 @@ __device__ __forceinline__ TwTables<T> stage_twiddles(cplx<T>* smem, const cplx<
   return t;
 }
 
+// the tables read in place from the device table [forward | inverse | quarter-wave]
+template <typename T, int N>
+__device__ __forceinline__ TwTables<T> device_twiddles(const cplx<T>* g) {
+  constexpr int nf = tw_size<N, -1>(), ni = tw_size<N, +1>();
+  TwTables<T> t;
+  t.f = g;
+  t.i = tw_shared<N>() ? g : g + nf;
+  t.d = g + nf + ni;
+  return t;
+}
+
 // element index held in register slot (b*R + r) after the last pass of
 // direction DIR (equivalently: loaded in that slot by the first pass of -DIR)
 template <int N, int DIR>

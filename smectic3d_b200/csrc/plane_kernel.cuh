@@ -94,7 +94,24 @@ struct PlaneCfg {
   static constexpr size_t SB_OFF = ALIAS ? 0 : LB_BYTES;
   static constexpr size_t RB_OFF = ALIAS ? REGION : SB_OFF + XB_BYTES;
   static constexpr size_t TW_OFF = RB_OFF + (ALIAS ? REGION : XB_BYTES);
-  static constexpr size_t MB_OFF = align_up(TW_OFF + size_t(TW_ENTRIES) * sizeof(cplx<T>), 16);
+  // CTAs per SM that shared memory admits for a CTA of ``bytes`` (228 KB per
+  // SM, 1 KB reserved per CTA)
+  static constexpr int ctas_by_smem(size_t bytes) { return int(233472 / (bytes + 1024)); }
+  static constexpr size_t smem_with(size_t tw_bytes) {
+    return align_up(TW_OFF + tw_bytes, 16) + 16 + RED_DOUBLES * sizeof(double);
+  }
+  // The twiddle tables are staged in shared memory unless reading them in place
+  // from the device table (through L1) lifts a shared-memory-bound CTA count of
+  // two or fewer per SM.  That is done for the FP64 cosine transforms only: their
+  // 7.9 KB of tables at 256^3 (clusters of 16) are what keeps a third CTA out,
+  // and three 128-thread CTAs of that kernel also fit the register file (ptxas:
+  // 168 registers); the FP64 periodic plane kernel is register-bound at two
+  // (192 registers) and only loses by reading its tables through L1.
+  static constexpr bool TW_SMEM =
+      !(sizeof(T) == 8 && DCT && ctas_by_smem(smem_with(size_t(TW_ENTRIES) * sizeof(cplx<T>))) <= 2 &&
+        ctas_by_smem(smem_with(0)) > ctas_by_smem(smem_with(size_t(TW_ENTRIES) * sizeof(cplx<T>))));
+  static constexpr size_t TW_BYTES = TW_SMEM ? size_t(TW_ENTRIES) * sizeof(cplx<T>) : 0;
+  static constexpr size_t MB_OFF = align_up(TW_OFF + TW_BYTES, 16);
   static constexpr size_t RED_OFF = MB_OFF + 16;
   static constexpr size_t SMEM = RED_OFF + RED_DOUBLES * sizeof(double);
   static constexpr bool fits = SMEM <= 227 * 1024;  // per-CTA shared memory limit of sm_100
@@ -867,7 +884,9 @@ plane_kernel(PlaneArgs<T> a) {
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);
   double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::RED_OFF);
   const TwTables<T> tw =
-      stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS, DCT);
+      Cfg::TW_SMEM
+          ? stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS, DCT)
+          : device_twiddles<T, N>(a.tw);
 
   int rank = 0;
   if constexpr (CL > 1) rank = int(cg::this_cluster().block_rank());

@@ -29,3 +29,15 @@ def test_residency_unclustered_counts_every_slot():
     assert r["plane_cluster"] == 1 and r["plane_ctas"] == 32 * 4
     assert r["plane_clusters_resident"] == r["plane_ctas_per_sm"] * r["sms"]
     assert r["pencil_ctas_per_sm"] >= 1
+
+
+def test_residency_256_fp64_neumann_reads_twiddles_in_place():
+    """FP64 Neumann 256^3 (clusters of 16): with its 7.9 KB of twiddles read from
+    the device table instead of shared memory, three CTAs fit an SM; the periodic
+    plane pass, register-bound at two, keeps them in shared memory."""
+    with S.Solver(S.Params(n=256, boundary="neumann", precision="fp64")) as s:
+        r = s.residency()
+    assert r["plane_cluster"] == 16 and r["plane_ctas_per_sm"] == 3
+    with S.Solver(S.Params(n=256, boundary="periodic", precision="fp64")) as s:
+        r = s.residency()
+    assert r["plane_cluster"] == 16 and r["plane_ctas_per_sm"] == 2
