@@ -251,6 +251,7 @@ pencil_kernel(PencilArgs<T> a) {
   double* scratch = reinterpret_cast<double*>(smem_raw + Cfg::red_off(MODE));
   const TwTables<T> tw =
       stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::tw_off(MODE)), a.tw, threadIdx.x, Cfg::THREADS, DCT);
+  __syncthreads();  // every staged entry is written before any thread's first transform (kPencilAdjOut starts with one)
   grid_dependency_wait();
 
   const int f0 = blockIdx.x * TK;

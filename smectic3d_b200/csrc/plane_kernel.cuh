@@ -887,6 +887,9 @@ plane_kernel(PlaneArgs<T> a) {
       Cfg::TW_SMEM
           ? stage_twiddles<T, N>(reinterpret_cast<cplx<T>*>(smem_raw + Cfg::TW_OFF), a.tw, threadIdx.x, Cfg::THREADS, DCT)
           : device_twiddles<T, N>(a.tw);
+  // every staged entry is written before any thread's first transform (the
+  // passes that start with a row transform read them right away)
+  if constexpr (Cfg::TW_SMEM) __syncthreads();
 
   int rank = 0;
   if constexpr (CL > 1) rank = int(cg::this_cluster().block_rank());
