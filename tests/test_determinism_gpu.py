@@ -69,3 +69,17 @@ def test_adjoint_is_bitwise_reproducible():
     for r in res[1:]:
         for x, y in zip(r, res[0]):
             assert np.array_equal(x, y)
+
+
+def test_batched_replicas_graph_runs_are_bitwise_reproducible():
+    b = 16
+    p = S.Params(n=64, batch=b, boundary="periodic", precision="fp32", dt=0.05, eps=-0.75,
+                 eps_per_replica=tuple(np.linspace(-0.9, -0.5, b)))
+    psi0 = S.ic.noise_batch(64, range(b))
+    outs = []
+    for _ in range(2):
+        with S.Solver(p) as s:
+            s.set_psi(psi0)
+            s.step(320)
+            outs.append(s.get_psi())
+    assert np.array_equal(outs[0], outs[1])
