@@ -177,6 +177,20 @@ struct PlaneArgs {
   int drop_exchange;  // test hook (see Xchg::drop)
 };
 
+// One launch of the plane pass.  The modes that turn independent fields to or
+// from real space (kPlaneInvReal, kPlaneInvMulFwd, kPlaneMulFwd) take up to
+// kPlaneComps argument sets and run one per blockIdx.z, so that the components
+// of a gradient, stress or velocity share one grid (one wave tail instead of
+// one per component); every other mode uses set 0.
+constexpr int kPlaneComps = 3;
+template <typename T>
+struct PlaneLaunch {
+  PlaneArgs<T> c[kPlaneComps];
+};
+__host__ __device__ constexpr bool plane_multi(int mode) {
+  return mode == kPlaneInvReal || mode == kPlaneInvMulFwd || mode == kPlaneMulFwd;
+}
+
 // Cluster barrier halves.  barrier.cluster arrive and wait alternate in every
 // thread; Xchg below tracks whether an arrive is outstanding.
 template <int CL>
@@ -875,7 +889,8 @@ __device__ __forceinline__ void row_nonlin(cplx<T> (&v)[Plan<N>::E], cplx<T>* L,
 
 template <typename T, int N, int CL, bool DCT, int MODE>
 __global__ void __launch_bounds__(PlaneCfg<T, N, CL, DCT>::THREADS, PlaneCfg<T, N, CL, DCT>::min_blocks(MODE))
-plane_kernel(PlaneArgs<T> a) {
+plane_kernel(const __grid_constant__ PlaneLaunch<T> pl) {
+  const PlaneArgs<T>& a = pl.c[plane_multi(MODE) ? blockIdx.z : 0];
   using Cfg = PlaneCfg<T, N, CL, DCT>;
   using Ops = PlaneOps<T, N, CL, DCT>;
   constexpr int E = Cfg::E, G = Cfg::G, LS = Cfg::LS, ROWS = Cfg::ROWS, FP = Cfg::FP;

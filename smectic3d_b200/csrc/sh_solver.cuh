@@ -362,8 +362,19 @@ struct Solver final : SolverBase {
 
   template <int MODE>
   int launch_plane(const PlaneArgs<T>& a, int reps = 0) {
+    return launch_plane_sets<MODE>(&a, 1, reps);
+  }
+  // ``ncomp`` argument sets in one grid (blockIdx.z), for the modes that take several
+  template <int MODE>
+  int launch_plane_sets(const PlaneArgs<T>* as, int ncomp, int reps = 0) {
+    if (ncomp < 1 || ncomp > kPlaneComps || (ncomp > 1 && !plane_multi(MODE))) {
+      err = "plane pass: unsupported number of argument sets";
+      return SH_EINVAL;
+    }
+    PlaneLaunch<T> pl{};
+    for (int i = 0; i < ncomp; ++i) pl.c[i] = as[i];
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(N * CL, reps > 0 ? reps : p.batch, 1);
+    cfg.gridDim = dim3(N * CL, reps > 0 ? reps : p.batch, ncomp);
     cfg.blockDim = dim3(PC::THREADS, 1, 1);
     cfg.dynamicSmemBytes = PC::SMEM;
     cfg.stream = stream;
@@ -383,7 +394,7 @@ struct Solver final : SolverBase {
     }
     cfg.attrs = attr;
     cfg.numAttrs = na;
-    SHB_CUDA(cudaLaunchKernelEx(&cfg, plane_fn<MODE>(), a));
+    SHB_CUDA(cudaLaunchKernelEx(&cfg, plane_fn<MODE>(), pl));
     ++launches;
     return SH_OK;
   }
@@ -703,31 +714,20 @@ struct Solver final : SolverBase {
       // sine transform (signed cosine pair), the projector in the pencil pass,
       // then N = beta psi^3 - gamma psi^5 - u . grad psi forward -> Nt
       int rc;
-      const cplx<T>* src[2] = {P, PSH};
-      const int out[2] = {0, 4};
-      for (int i = 0; i < 2; ++i) {
-        PlaneArgs<T> a = plane_args();
-        a.src = src[i];
-        a.real_out = R[out[i]];
-        if (i == 0) {
-          a.flags = diag;
-          a.psi_old = d_stash;
-          a.psi_out = d_stash;
-        }
-        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
-      }
+      if ((rc = psi_lpsi_real(diag))) return rc;
       grad_wall_kernel<T><<<dim3(4 * 148, p.batch), 256, 0, stream>>>(R[0], R[1], R[2], R[3], N,
                                                                         T(0.5 / p.dx));
       SHB_CUDA(cudaGetLastError());
       ++launches;
+      PlaneArgs<T> st[3];
       for (int c = 0; c < 3; ++c) {
-        PlaneArgs<T> a = plane_args();
-        a.real_in[0] = R[4];
-        a.real_in[1] = R[1 + c];
-        a.sign_axes = 7;
-        a.dst = S3[c];
-        if ((rc = launch_plane<kPlaneMulFwd>(a))) return rc;
+        st[c] = plane_args();
+        st[c].real_in[0] = R[4];
+        st[c].real_in[1] = R[1 + c];
+        st[c].sign_axes = 7;
+        st[c].dst = S3[c];
       }
+      if ((rc = launch_plane_sets<kPlaneMulFwd>(st, 3))) return rc;
       PencilArgs<T> b = pencil_args();
       for (int c = 0; c < 3; ++c) {
         b.s3[c] = S3[c];
@@ -745,32 +745,20 @@ struct Solver final : SolverBase {
       return SH_OK;
     } else {
       int rc;
-      // psi and L psi to real space
-      const cplx<T>* src[2] = {P, PSH};
-      const int out[2] = {0, 4};
-      for (int i = 0; i < 2; ++i) {
-        PlaneArgs<T> a = plane_args();
-        a.src = src[i];
-        a.real_out = R[out[i]];
-        if (i == 0) {
-          a.flags = diag;
-          a.psi_old = d_stash;
-          a.psi_out = d_stash;
-        }
-        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
-      }
+      if ((rc = psi_lpsi_real(diag))) return rc;
       // grad psi to real space, and in the same pass the stress S_c = (L psi) d_c psi forward
       const cplx<T>* dsrc[3] = {Px, P, P};
       const int dmult[3] = {kMulNone, kMulIqy, kMulIqz};
+      PlaneArgs<T> st[3];
       for (int c = 0; c < 3; ++c) {
-        PlaneArgs<T> a = plane_args();
-        a.src = dsrc[c];
-        a.mult = dmult[c];
-        a.real_out = R[1 + c];
-        a.real_in[0] = R[4];
-        a.dst = S3[c];
-        if ((rc = launch_plane<kPlaneInvMulFwd>(a))) return rc;
+        st[c] = plane_args();
+        st[c].src = dsrc[c];
+        st[c].mult = dmult[c];
+        st[c].real_out = R[1 + c];
+        st[c].real_in[0] = R[4];
+        st[c].dst = S3[c];
       }
+      if ((rc = launch_plane_sets<kPlaneInvMulFwd>(st, 3))) return rc;
       PencilArgs<T> b = pencil_args();
       for (int c = 0; c < 3; ++c) {
         b.s3[c] = S3[c];
@@ -788,16 +776,30 @@ struct Solver final : SolverBase {
       return SH_OK;
     }
   }
+  // psi and L psi of the state held in P, PSH to real space (R[0], R[4]), one
+  // grid; the diagnostics ``diag`` (L1 monitor, psi stash) ride on psi
+  int psi_lpsi_real(int diag) {
+    PlaneArgs<T> st[2] = {plane_args(), plane_args()};
+    st[0].src = P;
+    st[0].real_out = R[0];
+    st[0].flags = diag;
+    st[0].psi_old = d_stash;
+    st[0].psi_out = d_stash;
+    st[1].src = PSH;
+    st[1].real_out = R[4];
+    return launch_plane_sets<kPlaneInvReal>(st, 2);
+  }
   // velocity of the current state in real space (R[5..7]) from its partials in S3
   int velocity_real() {
     int rc;
+    PlaneArgs<T> st[3];
     for (int c = 0; c < 3; ++c) {
-      PlaneArgs<T> a = plane_args();
-      a.src = S3[c];
-      a.real_out = R[5 + c];
-      a.sign_axes = DCT ? 7 : 0;  // Neumann: the partials carry (-1)^(x+y+z) u
-      if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+      st[c] = plane_args();
+      st[c].src = S3[c];
+      st[c].real_out = R[5 + c];
+      st[c].sign_axes = DCT ? 7 : 0;  // Neumann: the partials carry (-1)^(x+y+z) u
     }
+    if ((rc = launch_plane_sets<kPlaneInvReal>(st, 3))) return rc;
     u_real_current = true;
     return SH_OK;
   }
@@ -1212,13 +1214,14 @@ struct Solver final : SolverBase {
       // psi, psi_yy, psi_zz from the partial of psi; psi_xx and L psi through an x multiplier
       const int mult[3] = {kMulNone, kMulNegQy2, kMulNegQz2};
       T* outs[3] = {CR[0], CR[2], CR[3]};
+      PlaneArgs<T> st[3];
       for (int i = 0; i < 3; ++i) {
-        PlaneArgs<T> a = plane_args();
-        a.src = P;
-        a.mult = mult[i];
-        a.real_out = outs[i];
-        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+        st[i] = plane_args();
+        st[i].src = P;
+        st[i].mult = mult[i];
+        st[i].real_out = outs[i];
       }
+      if ((rc = launch_plane_sets<kPlaneInvReal>(st, 3))) return rc;
       const int xm[2] = {kXNegQx2, kXOpSH};
       T* xo[2] = {CR[1], CR[4]};
       for (int i = 0; i < 2; ++i) {
