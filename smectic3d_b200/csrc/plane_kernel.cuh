@@ -131,8 +131,10 @@ struct PlaneCfg {
        (SMEM + 1024) * MIN_BLOCKS_RAW <= 233472)
           ? MIN_BLOCKS_RAW
           : 0;
-  // kPlaneAdvN keeps an accumulator beside the transform registers: no cap
-  static constexpr int min_blocks(int mode) { return mode == kPlaneAdvN ? 0 : MIN_BLOCKS; }
+  // kPlaneAdvN keeps an accumulator beside the transform registers: capped for
+  // the periodic box (three CTAs per SM, small spills: 256^3 FP32 advected
+  // step -19 us), uncapped for the Neumann box, where the cap measured slower
+  static constexpr int min_blocks(int mode) { return (mode == kPlaneAdvN && DCT) ? 0 : MIN_BLOCKS; }
   static_assert(THREADS % 32 == 0, "plane CTA must be whole warps");
 };
 

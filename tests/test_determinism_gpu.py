@@ -83,3 +83,22 @@ def test_batched_replicas_graph_runs_are_bitwise_reproducible():
             s.step(320)
             outs.append(s.get_psi())
     assert np.array_equal(outs[0], outs[1])
+
+
+def test_advected_neumann_256_fp64_is_bitwise_reproducible():
+    """FP64 cosine plane passes at 256^3 read their twiddles through L1 (no staging)."""
+    p = S.Params(n=256, boundary="neumann", precision="fp64", dt=0.05, eps=-0.75, advection=True)
+    _lockstep(p, S.ic.noise(256, 4), steps=20, every=10)
+
+
+def test_surface_step_is_bitwise_reproducible():
+    p = S.Params(n=256, boundary="periodic", precision="fp32", dt=0.05, eps=-0.75, advection=True)
+    psi0 = S.ic.noise(256, 5)
+    outs = []
+    for _ in range(2):
+        with S.Solver(p) as s:
+            s.set_psi(psi0)
+            s.step(3)
+            outs.append(s.surface_step())
+    for x, y in zip(outs[0], outs[1]):
+        assert np.array_equal(x, y, equal_nan=True) if x.dtype.kind == "f" else np.array_equal(x, y)
