@@ -66,7 +66,8 @@ typedef struct sh_params {
   int precision;     /* SH_FP64 / SH_FP32                                    */
   int l1_interval;   /* steps between L1 evaluations (pf3d.cpp:489: 100); 0 = off */
   int energy_trace;  /* 1: record the energy of every new state              */
-  int variant;       /* kernel shape override (0 = default; see sh_variants)  */
+  int variant;       /* plane-pass cluster size (0 = default; built: 1, 2 at 64^3;
+                        1, 2, 4 at 128^3; 4, 8, 16 at 256^3; 16 at 512^3)     */
   double dx, dt, eps, beta, gamma, alpha, q0, eta, rho;
   double w_mid;      /* pinning penalty weight (periodicFFT/pf3dMorph.cpp:102) */
   double sub_sigma;  /* substrate penalty sigma (cosFFT/comet/cosNoAdvMorph.cpp:67-74) */
@@ -75,6 +76,8 @@ typedef struct sh_params {
   int curvature;     /* Neumann curvature pass: SH_CURV_DIFFERENCE / SH_CURV_SPECTRAL */
   int replica_block; /* batched plain steps: replicas advanced together, 16 steps at a
                         time, while their state stays in L2 (0 = all replicas each step) */
+  int pencil_tile;   /* lines per CTA of the pencil (x) pass: 0 = the default (16 FP32,
+                        8 FP64); 8, 16 and 32 are built at 64^3, the batched replicas' size */
 } sh_params;
 
 typedef struct sh_handle sh_handle;

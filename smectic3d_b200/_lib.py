@@ -37,6 +37,7 @@ class ShParams(C.Structure):
         ("gamma", C.c_double), ("alpha", C.c_double), ("q0", C.c_double), ("eta", C.c_double),
         ("rho", C.c_double), ("w_mid", C.c_double), ("sub_sigma", C.c_double), ("sub_z0", C.c_double),
         ("eps_per_replica", C.POINTER(C.c_double)), ("curvature", C.c_int), ("replica_block", C.c_int),
+        ("pencil_tile", C.c_int),
     ]
 
 

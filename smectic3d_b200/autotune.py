@@ -10,9 +10,13 @@ advance together, 16 steps at a time, while their state stays in the 126 MB L2
 (0: every replica each step).  A block whose CTAs fill the GPU in about one wave
 and whose fields fit L2 wins.
 
+At 64^3 the pencil pass is also built with tiles of 8, 16 and 32 lines per CTA
+(``pencil_tile``): smaller tiles mean more, smaller CTAs.
+
 The tuner times a few steps of every built candidate for a given (n, batch,
 boundary, precision, advection), first the cluster size, then the replica
-block with that cluster size, and keeps the fastest. Results are cached in a
+block with that cluster size, then the pencil tile with both, and keeps the
+fastest. Results are cached in a
 JSON file keyed by that tuple and by the GPU name, under
 $SMECTIC_B200_CACHE (default ~/.cache/smectic3d_b200/tuned.json).
 """
@@ -29,6 +33,8 @@ import numpy as np
 CANDIDATES = {16: (1,), 32: (1,), 64: (1, 2), 128: (1, 2, 4), 256: (4, 8, 16), 512: (16,)}
 # replicas per L2-resident block, tried for batched plain runs at n <= 128
 BLOCKS = (4, 8, 12, 13, 16, 21, 32)
+# pencil tiles (lines per CTA) built besides the default
+TILES = {64: (8, 16, 32)}
 
 
 def cache_path() -> Path:
@@ -100,6 +106,18 @@ def tune(p, steps: int = 32, use_cache: bool = True) -> dict:
                 continue
         rec["replica_block"] = min(bt, key=bt.get)
         rec["us_per_step_by_block"] = {str(k): v for k, v in bt.items()}
+    rec["pencil_tile"] = 0
+    tiles = TILES.get(p.n, ())
+    if tiles:
+        blk = rec["replica_block"]
+        tt = {0: rec.get("us_per_step_by_block", {}).get(str(blk), times[best])}
+        for tk in tiles:
+            try:
+                tt[tk] = _time_variant(dataclasses.replace(p, replica_block=blk, pencil_tile=tk), best, steps) * 1e6
+            except Exception:  # the default tile again, or not built
+                continue
+        rec["pencil_tile"] = min(tt, key=tt.get)
+        rec["us_per_step_by_tile"] = {str(k): v for k, v in tt.items()}
     cache[key] = rec
     path.parent.mkdir(parents=True, exist_ok=True)
     path.write_text(json.dumps(cache, indent=1, sort_keys=True))
@@ -114,3 +132,11 @@ def best_config(p) -> tuple[int, int]:
     """(variant, replica_block) of the fastest tuned configuration."""
     rec = tune(p)
     return int(rec["variant"]), int(rec.get("replica_block", 0))
+
+
+def best_shape(p) -> dict:
+    """Params fields of the fastest tuned configuration: variant, replica_block,
+    pencil_tile."""
+    rec = tune(p)
+    return {"variant": int(rec["variant"]), "replica_block": int(rec.get("replica_block", 0)),
+            "pencil_tile": int(rec.get("pencil_tile", 0))}

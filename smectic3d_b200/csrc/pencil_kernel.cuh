@@ -55,11 +55,12 @@ __host__ __device__ constexpr int pencil_sets(int mode) {
   return mode == kPencilStokes ? 3 : ((mode == kPencilStepAdv || mode == kPencilInitAdv) ? 2 : 1);
 }
 
-template <typename T, int N, bool DCT>
+// TKV: lines per CTA (the tile), 0 = the default of 16 (FP32) or 8 (FP64)
+template <typename T, int N, bool DCT, int TKV = 0>
 struct PencilCfg {
   static constexpr int E = Plan<N>::E;
   static constexpr int G = N / E;
-  static constexpr int TK = sizeof(T) == 4 ? 16 : 8;
+  static constexpr int TK = TKV > 0 ? TKV : (sizeof(T) == 4 ? 16 : 8);
   static constexpr int THREADS = TK * G;
   static constexpr int LS = line_stride(N);
   static constexpr int FP = DCT ? N * (N / 2) : N * (N / 2 + 1);
@@ -118,9 +119,9 @@ struct PencilArgs {
   int flags;
 };
 
-template <typename T, int N, bool DCT>
+template <typename T, int N, bool DCT, int TKV = 0>
 struct PencilOps {
-  using Cfg = PencilCfg<T, N, DCT>;
+  using Cfg = PencilCfg<T, N, DCT, TKV>;
   static constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
 
   // the TK lines of a tile are consecutive in memory (f0 and TK even: 16-byte pairs)
@@ -240,11 +241,11 @@ __device__ __forceinline__ Mult<T> make_mult(T qx, T qy, T qz, T eps, const Poin
 __device__ __forceinline__ float rcp_rn(float x) { return __frcp_rn(x); }
 __device__ __forceinline__ double rcp_rn(double x) { return __drcp_rn(x); }
 
-template <typename T, int N, bool DCT, int MODE>
-__global__ void __launch_bounds__(PencilCfg<T, N, DCT>::THREADS, PencilCfg<T, N, DCT>::min_blocks(MODE))
+template <typename T, int N, bool DCT, int MODE, int TKV = 0>
+__global__ void __launch_bounds__(PencilCfg<T, N, DCT, TKV>::THREADS, PencilCfg<T, N, DCT, TKV>::min_blocks(MODE))
 pencil_kernel(PencilArgs<T> a) {
-  using Cfg = PencilCfg<T, N, DCT>;
-  using Ops = PencilOps<T, N, DCT>;
+  using Cfg = PencilCfg<T, N, DCT, TKV>;
+  using Ops = PencilOps<T, N, DCT, TKV>;
   constexpr int E = Cfg::E, G = Cfg::G, TK = Cfg::TK, LS = Cfg::LS, FP = Cfg::FP, RL = Cfg::RL;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cplx<T>* buf = reinterpret_cast<cplx<T>*>(smem_raw);

@@ -180,6 +180,7 @@ int sh_default_params(sh_params* p) {
   p->eps_per_replica = nullptr;
   p->curvature = SH_CURV_DIFFERENCE;
   p->replica_block = 0;
+  p->pencil_tile = 0;
   return SH_OK;
 }
 
@@ -205,13 +206,16 @@ int sh_create(const sh_params* p, sh_handle** out) {
   if (p->curvature != SH_CURV_DIFFERENCE && p->curvature != SH_CURV_SPECTRAL)
     return fail(nullptr, SH_EINVAL, "bad curvature");
   if (p->replica_block < 0) return fail(nullptr, SH_EINVAL, "replica_block must be >= 0");
+  if (p->pencil_tile != 0 && p->pencil_tile != 8 && p->pencil_tile != 16 && p->pencil_tile != 32)
+    return fail(nullptr, SH_EINVAL, "pencil_tile must be 0, 8, 16 or 32");
 
   SolverBase* s = nullptr;
   const bool f32 = p->precision != SH_FP64;
+  const int tile = p->pencil_tile;
   if (p->boundary == SH_PERIODIC)
-    s = f32 ? make_solver_f32_periodic(p->n, p->variant) : make_solver_f64_periodic(p->n, p->variant);
+    s = f32 ? make_solver_f32_periodic(p->n, p->variant, tile) : make_solver_f64_periodic(p->n, p->variant, tile);
   else
-    s = f32 ? make_solver_f32_neumann(p->n, p->variant) : make_solver_f64_neumann(p->n, p->variant);
+    s = f32 ? make_solver_f32_neumann(p->n, p->variant, tile) : make_solver_f64_neumann(p->n, p->variant, tile);
   if (!s) return fail(nullptr, SH_EUNSUPPORTED, "this size / variant is not built");
   std::unique_ptr<sh_handle> h(new sh_handle);
   h->s = s;

@@ -8,23 +8,45 @@ namespace shb {
 // Cluster size CL of the plane pass (NC = N / (2 CL) column lines per CTA).
 // ``variant`` selects a CL explicitly (0 = default); a CL whose working set
 // does not fit one CTA's shared memory is not built.
-template <typename T, int N, int CL, bool DCT>
+template <typename T, int N, int CL, bool DCT, int TKV = 0>
 SolverBase* make_if_fits() {
   if constexpr (PlaneCfg<T, N, CL, DCT>::fits) {
-    return new Solver<T, N, CL, DCT>();
+    return new Solver<T, N, CL, DCT, TKV>();
   } else {
     return nullptr;
   }
 }
 
-// Solver of one grid size N with cluster size ``cl`` (0 = the default).
+// 64^3 (the batched replicas' size): pencil tiles of 8, 16 or 32 lines per CTA
+// (``tile``, 0 = the default), with the plane cluster size ``CL``
+template <typename T, int CL, bool DCT>
+SolverBase* make_tiled_64(int tile) {
+  constexpr int def = PencilCfg<T, 64, DCT>::TK;
+  if (tile == 0 || tile == def) return make_if_fits<T, 64, CL, DCT>();
+  if constexpr (def != 8) {
+    if (tile == 8) return make_if_fits<T, 64, CL, DCT, 8>();
+  }
+  if constexpr (def != 16) {
+    if (tile == 16) return make_if_fits<T, 64, CL, DCT, 16>();
+  }
+  if constexpr (def != 32) {
+    if (tile == 32) return make_if_fits<T, 64, CL, DCT, 32>();
+  }
+  return nullptr;
+}
+
+// Solver of one grid size N with cluster size ``cl`` (0 = the default) and
+// pencil tile ``tile`` (0 = the default; other tiles are built at 64^3 only).
 template <typename T, int N, bool DCT>
-SolverBase* make_sized(int cl) {
+SolverBase* make_sized(int cl, int tile) {
+  if constexpr (N != 64) {
+    if (tile != 0 && tile != PencilCfg<T, N, DCT>::TK) return nullptr;
+  }
   if constexpr (N <= 32) {
     return cl == 0 || cl == 1 ? make_if_fits<T, N, 1, DCT>() : nullptr;
   } else if constexpr (N == 64) {
-    if (cl == 0 || cl == 1) return make_if_fits<T, 64, 1, DCT>();
-    if (cl == 2) return make_if_fits<T, 64, 2, DCT>();
+    if (cl == 0 || cl == 1) return make_tiled_64<T, 1, DCT>(tile);
+    if (cl == 2) return make_tiled_64<T, 2, DCT>(tile);
     return nullptr;
   } else if constexpr (N == 128) {
     if (cl == 0 || cl == 1) return make_if_fits<T, 128, 1, DCT>();
@@ -51,5 +73,5 @@ SolverBase* make_sized(int cl) {
 // defines shb::make_solver_f32_neumann_n256.
 #define SHB_INST_UNIT(P, B, T, DCT, N) \
   namespace shb {                       \
-  SolverBase* make_solver_##P##_##B##_n##N(int cl) { return make_sized<T, N, DCT>(cl); } \
+  SolverBase* make_solver_##P##_##B##_n##N(int cl, int tile) { return make_sized<T, N, DCT>(cl, tile); } \
   }

@@ -146,10 +146,10 @@ struct SolverBase {
   virtual int residency(int* out) = 0;
 };
 
-template <typename T, int N, int CL, bool DCT>
+template <typename T, int N, int CL, bool DCT, int TKV = 0>
 struct Solver final : SolverBase {
   using PC = PlaneCfg<T, N, CL, DCT>;
-  using QC = PencilCfg<T, N, DCT>;
+  using QC = PencilCfg<T, N, DCT, TKV>;
   static constexpr int FP = PC::FP;
   // step kernels may start while the previous kernel drains (SMECTIC_B200_NO_PDL=1: off)
   bool use_pdl = getenv("SMECTIC_B200_NO_PDL") == nullptr;
@@ -251,7 +251,7 @@ struct Solver final : SolverBase {
   template <int MODE>
   static constexpr auto plane_fn() { return &plane_kernel<T, N, CL, DCT, MODE>; }
   template <int MODE>
-  static constexpr auto pencil_fn() { return &pencil_kernel<T, N, DCT, MODE>; }
+  static constexpr auto pencil_fn() { return &pencil_kernel<T, N, DCT, MODE, TKV>; }
 
   template <class K>
   int set_attrs(K kern, size_t smem, bool cluster) {
@@ -1325,20 +1325,20 @@ struct Solver final : SolverBase {
 // factories: one per (precision, boundary, size), defined in the
 // instantiation units sh_inst_<precision>_<boundary>_<size>.cu
 #define SHB_DECLARE_FACTORIES(P, B)                                                                  \
-  SolverBase* make_solver_##P##_##B##_n16(int cl);                                                   \
-  SolverBase* make_solver_##P##_##B##_n32(int cl);                                                   \
-  SolverBase* make_solver_##P##_##B##_n64(int cl);                                                   \
-  SolverBase* make_solver_##P##_##B##_n128(int cl);                                                  \
-  SolverBase* make_solver_##P##_##B##_n256(int cl);                                                  \
-  SolverBase* make_solver_##P##_##B##_n512(int cl);                                                  \
-  inline SolverBase* make_solver_##P##_##B(int n, int variant) {                                     \
+  SolverBase* make_solver_##P##_##B##_n16(int cl, int tile);                                         \
+  SolverBase* make_solver_##P##_##B##_n32(int cl, int tile);                                         \
+  SolverBase* make_solver_##P##_##B##_n64(int cl, int tile);                                         \
+  SolverBase* make_solver_##P##_##B##_n128(int cl, int tile);                                        \
+  SolverBase* make_solver_##P##_##B##_n256(int cl, int tile);                                        \
+  SolverBase* make_solver_##P##_##B##_n512(int cl, int tile);                                        \
+  inline SolverBase* make_solver_##P##_##B(int n, int variant, int tile) {                           \
     switch (n) {                                                                                      \
-      case 16: return make_solver_##P##_##B##_n16(variant);                                          \
-      case 32: return make_solver_##P##_##B##_n32(variant);                                          \
-      case 64: return make_solver_##P##_##B##_n64(variant);                                          \
-      case 128: return make_solver_##P##_##B##_n128(variant);                                        \
-      case 256: return make_solver_##P##_##B##_n256(variant);                                        \
-      case 512: return make_solver_##P##_##B##_n512(variant);                                        \
+      case 16: return make_solver_##P##_##B##_n16(variant, tile);                                    \
+      case 32: return make_solver_##P##_##B##_n32(variant, tile);                                    \
+      case 64: return make_solver_##P##_##B##_n64(variant, tile);                                    \
+      case 128: return make_solver_##P##_##B##_n128(variant, tile);                                  \
+      case 256: return make_solver_##P##_##B##_n256(variant, tile);                                  \
+      case 512: return make_solver_##P##_##B##_n512(variant, tile);                                  \
       default: return nullptr;                                                                        \
     }                                                                                                 \
   }

@@ -44,6 +44,7 @@ class Params:
     variant: int = 0                 # plane-pass cluster size (0 = default, -1 = autotune)
     curvature: str = "difference"    # Neumann curvature pass: "difference" (reference) | "spectral"
     replica_block: int = 0           # batched plain steps: replicas per L2-resident block (0 = off)
+    pencil_tile: int = 0             # lines per pencil CTA (0 = default; 8, 16, 32 at 64^3)
 
     @staticmethod
     def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":
@@ -63,6 +64,7 @@ class Params:
         p.variant = int(self.variant)
         p.curvature = {"difference": L.SH_CURV_DIFFERENCE, "spectral": L.SH_CURV_SPECTRAL}[self.curvature]
         p.replica_block = int(self.replica_block)
+        p.pencil_tile = int(self.pencil_tile)
         for k in ("dx", "dt", "eps", "beta", "gamma", "alpha", "q0", "eta", "rho", "w_mid", "sub_sigma", "sub_z0"):
             setattr(p, k, float(getattr(self, k)))
         keep = None
@@ -78,9 +80,8 @@ class Solver:
     def __init__(self, params: Params):
         self.lib = L.load()
         if params.variant < 0:
-            from .autotune import best_config
-            v, blk = best_config(dataclasses.replace(params, variant=0))
-            params = dataclasses.replace(params, variant=v, replica_block=blk)
+            from .autotune import best_shape
+            params = dataclasses.replace(params, **best_shape(dataclasses.replace(params, variant=0)))
         self.params = params
         cp, keep = params.to_c()
         h = C.c_void_p()

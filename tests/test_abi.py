@@ -40,9 +40,9 @@ def test_params_struct_layout_matches_header():
 #include <stddef.h>
 #include "smectic_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(sh_params), offsetof(sh_params, dx), offsetof(sh_params, w_mid),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(sh_params), offsetof(sh_params, dx), offsetof(sh_params, w_mid),
          offsetof(sh_params, sub_z0), offsetof(sh_params, eps_per_replica), offsetof(sh_params, curvature),
-         offsetof(sh_params, replica_block));
+         offsetof(sh_params, replica_block), offsetof(sh_params, pencil_tile));
   return 0;
 }
 """
@@ -55,7 +55,7 @@ int main(void) {
     got = [int(v) for v in out]
     P = L.ShParams
     assert got == [C.sizeof(P), P.dx.offset, P.w_mid.offset, P.sub_z0.offset, P.eps_per_replica.offset,
-                   P.curvature.offset, P.replica_block.offset]
+                   P.curvature.offset, P.replica_block.offset, P.pencil_tile.offset]
 
 
 def test_default_params(lib):
@@ -78,6 +78,8 @@ def test_default_params(lib):
         ("dt", -1.0, L.SH_EINVAL),
         ("dx", 0.0, L.SH_EINVAL),
         ("l1_interval", -2, L.SH_EINVAL),
+        ("pencil_tile", 12, L.SH_EINVAL),
+        ("pencil_tile", 32, L.SH_EUNSUPPORTED),  # tiles other than the default are built at 64^3 only
     ],
 )
 def test_create_rejects_bad_params(lib, field, value, code):

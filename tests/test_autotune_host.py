@@ -86,3 +86,23 @@ def test_replica_block_is_tuned_for_batched_runs(fake, monkeypatch):
     seen.clear()
     rec = autotune.tune(S.Params(n=64, precision="fp32", batch=1), steps=3)
     assert rec["replica_block"] == 0 and all(b == 0 for _, b in seen)
+
+
+def test_pencil_tile_is_tuned_at_64(fake, monkeypatch):
+    """At 64^3 the tuner then tries the pencil tiles with the best cluster size
+    and replica block; best_shape returns all three Params fields."""
+    seen = []
+
+    def _time_variant(p, v, steps):
+        seen.append((v, p.replica_block, p.pencil_tile))
+        return ({1: 100.0, 2: 120.0}[v] - (30.0 if p.pencil_tile == 32 else 0.0)) * 1e-6
+    monkeypatch.setattr(autotune, "_time_variant", _time_variant)
+    p = S.Params(n=64, precision="fp32", batch=1)
+    rec = autotune.tune(p, steps=3)
+    assert rec["variant"] == 1 and rec["pencil_tile"] == 32
+    assert {t for _, _, t in seen[2:]} == {8, 16, 32} and all(v == 1 for v, _, _ in seen[2:])
+    assert autotune.best_shape(p) == {"variant": 1, "replica_block": 0, "pencil_tile": 32}
+    # sizes without tile variants keep the default
+    seen.clear()
+    monkeypatch.setattr(autotune, "_time_variant", lambda p, v, steps: {1: 1e-5, 2: 2e-5, 4: 3e-5}[v])
+    assert autotune.tune(S.Params(n=128, precision="fp64"), steps=3)["pencil_tile"] == 0
