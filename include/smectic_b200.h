@@ -77,7 +77,8 @@ typedef struct sh_params {
   int replica_block; /* batched plain steps: replicas advanced together, 16 steps at a
                         time, while their state stays in L2 (0 = all replicas each step) */
   int pencil_tile;   /* lines per CTA of the pencil (x) pass: 0 = the default (16 FP32,
-                        8 FP64); 8, 16 and 32 are built at 64^3, the batched replicas' size */
+                        8 FP64); 8, 16 and 32 are built at 64^3 and at 128^3 with
+                        variant 0 or 1 */
 } sh_params;
 
 typedef struct sh_handle sh_handle;

@@ -10,8 +10,9 @@ advance together, 16 steps at a time, while their state stays in the 126 MB L2
 (0: every replica each step).  A block whose CTAs fill the GPU in about one wave
 and whose fields fit L2 wins.
 
-At 64^3 the pencil pass is also built with tiles of 8, 16 and 32 lines per CTA
-(``pencil_tile``): smaller tiles mean more, smaller CTAs.
+At 64^3, and at 128^3 with cluster size 1, the pencil pass is also built with
+tiles of 8, 16 and 32 lines per CTA (``pencil_tile``): smaller tiles mean more,
+smaller CTAs.
 
 The tuner times a few steps of every built candidate for a given (n, batch,
 boundary, precision, advection), first the cluster size, then the replica
@@ -34,7 +35,7 @@ CANDIDATES = {16: (1,), 32: (1,), 64: (1, 2), 128: (1, 2, 4), 256: (4, 8, 16), 5
 # replicas per L2-resident block, tried for batched plain runs at n <= 128
 BLOCKS = (4, 8, 12, 13, 16, 21, 32)
 # pencil tiles (lines per CTA) built besides the default
-TILES = {64: (8, 16, 32)}
+TILES = {64: (8, 16, 32), 128: (8, 16, 32)}
 
 
 def cache_path() -> Path:

@@ -17,39 +17,40 @@ SolverBase* make_if_fits() {
   }
 }
 
-// 64^3 (the batched replicas' size): pencil tiles of 8, 16 or 32 lines per CTA
-// (``tile``, 0 = the default), with the plane cluster size ``CL``
-template <typename T, int CL, bool DCT>
-SolverBase* make_tiled_64(int tile) {
-  constexpr int def = PencilCfg<T, 64, DCT>::TK;
-  if (tile == 0 || tile == def) return make_if_fits<T, 64, CL, DCT>();
+// Pencil tiles of 8, 16 or 32 lines per CTA (``tile``, 0 = the default), with
+// the plane cluster size ``CL``: built for the batched replicas' 64^3 and for
+// 128^3 without clusters
+template <typename T, int N, int CL, bool DCT>
+SolverBase* make_tiled(int tile) {
+  constexpr int def = PencilCfg<T, N, DCT>::TK;
+  if (tile == 0 || tile == def) return make_if_fits<T, N, CL, DCT>();
   if constexpr (def != 8) {
-    if (tile == 8) return make_if_fits<T, 64, CL, DCT, 8>();
+    if (tile == 8) return make_if_fits<T, N, CL, DCT, 8>();
   }
   if constexpr (def != 16) {
-    if (tile == 16) return make_if_fits<T, 64, CL, DCT, 16>();
+    if (tile == 16) return make_if_fits<T, N, CL, DCT, 16>();
   }
   if constexpr (def != 32) {
-    if (tile == 32) return make_if_fits<T, 64, CL, DCT, 32>();
+    if (tile == 32) return make_if_fits<T, N, CL, DCT, 32>();
   }
   return nullptr;
 }
 
 // Solver of one grid size N with cluster size ``cl`` (0 = the default) and
-// pencil tile ``tile`` (0 = the default; other tiles are built at 64^3 only).
+// pencil tile ``tile`` (0 = the default; other tiles at 64^3, and at 128^3 with
+// cluster size 1).
 template <typename T, int N, bool DCT>
 SolverBase* make_sized(int cl, int tile) {
-  if constexpr (N != 64) {
-    if (tile != 0 && tile != PencilCfg<T, N, DCT>::TK) return nullptr;
-  }
+  const bool other_tile = tile != 0 && tile != PencilCfg<T, N, DCT>::TK;
+  if (other_tile && !(N == 64 || (N == 128 && cl <= 1))) return nullptr;
   if constexpr (N <= 32) {
     return cl == 0 || cl == 1 ? make_if_fits<T, N, 1, DCT>() : nullptr;
   } else if constexpr (N == 64) {
-    if (cl == 0 || cl == 1) return make_tiled_64<T, 1, DCT>(tile);
-    if (cl == 2) return make_tiled_64<T, 2, DCT>(tile);
+    if (cl == 0 || cl == 1) return make_tiled<T, 64, 1, DCT>(tile);
+    if (cl == 2) return make_tiled<T, 64, 2, DCT>(tile);
     return nullptr;
   } else if constexpr (N == 128) {
-    if (cl == 0 || cl == 1) return make_if_fits<T, 128, 1, DCT>();
+    if (cl == 0 || cl == 1) return make_tiled<T, 128, 1, DCT>(tile);
     if (cl == 2) return make_if_fits<T, 128, 2, DCT>();
     if (cl == 4) return make_if_fits<T, 128, 4, DCT>();
     return nullptr;

@@ -44,7 +44,7 @@ class Params:
     variant: int = 0                 # plane-pass cluster size (0 = default, -1 = autotune)
     curvature: str = "difference"    # Neumann curvature pass: "difference" (reference) | "spectral"
     replica_block: int = 0           # batched plain steps: replicas per L2-resident block (0 = off)
-    pencil_tile: int = 0             # lines per pencil CTA (0 = default; 8, 16, 32 at 64^3)
+    pencil_tile: int = 0             # lines per pencil CTA (0 = default; 8, 16, 32 at 64^3 and 128^3)
 
     @staticmethod
     def from_nw(n: int, nw: int, q0: float = 1.0, **kw) -> "Params":

@@ -79,7 +79,6 @@ def test_default_params(lib):
         ("dx", 0.0, L.SH_EINVAL),
         ("l1_interval", -2, L.SH_EINVAL),
         ("pencil_tile", 12, L.SH_EINVAL),
-        ("pencil_tile", 32, L.SH_EUNSUPPORTED),  # tiles other than the default are built at 64^3 only
     ],
 )
 def test_create_rejects_bad_params(lib, field, value, code):
@@ -161,3 +160,14 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(L, "LIB_PATH", tmp_path / "libsmectic_b200.so")
     with pytest.raises(ImportError, match="is missing"):
         L.load()
+
+
+def test_pencil_tiles_are_built_at_64_and_128_only(lib):
+    """Tiles other than the default exist at 64^3 and at 128^3 without clusters."""
+    for n, variant in ((256, 0), (128, 2), (32, 0)):
+        p = L.ShParams()
+        lib.sh_default_params(C.byref(p))
+        p.n, p.variant, p.pencil_tile = n, variant, 32
+        h = C.c_void_p()
+        assert lib.sh_create(C.byref(p), C.byref(h)) == L.SH_EUNSUPPORTED, (n, variant)
+        assert not h.value

@@ -104,5 +104,5 @@ def test_pencil_tile_is_tuned_at_64(fake, monkeypatch):
     assert autotune.best_shape(p) == {"variant": 1, "replica_block": 0, "pencil_tile": 32}
     # sizes without tile variants keep the default
     seen.clear()
-    monkeypatch.setattr(autotune, "_time_variant", lambda p, v, steps: {1: 1e-5, 2: 2e-5, 4: 3e-5}[v])
-    assert autotune.tune(S.Params(n=128, precision="fp64"), steps=3)["pencil_tile"] == 0
+    monkeypatch.setattr(autotune, "_time_variant", lambda p, v, steps: {4: 1e-5, 8: 2e-5, 16: 3e-5}[v])
+    assert autotune.tune(S.Params(n=256, precision="fp64"), steps=3)["pencil_tile"] == 0
