@@ -177,6 +177,9 @@ struct PlaneArgs {
   // (reversed coefficients -q_{N-k} X[N-k], 0 at k = 0)
   int sin_dz;
   int drop_exchange;  // test hook (see Xchg::drop)
+  // > 0: rank 0 of the cluster of plane x starts bringing plane x + pf_dist of
+  // the column input into L2 (the plane a cluster of a later wave loads first)
+  int pf_dist;
 };
 
 // One launch of the plane pass.  The modes that turn independent fields to or
@@ -933,6 +936,17 @@ plane_kernel(const __grid_constant__ PlaneLaunch<T> pl) {
   }
   grid_dependency_wait();
   const int x = blockIdx.x / CL;
+  if (a.pf_dist > 0 && rank == 0 && threadIdx.x == 0 && x + a.pf_dist < N) {
+    const size_t off = (size_t(blockIdx.y) * N + x + a.pf_dist) * FP;
+    const uint32_t bytes = uint32_t(size_t(FP) * sizeof(cplx<T>));
+    if constexpr (MODE == kPlaneStep || MODE == kPlaneGetPsi || MODE == kPlaneInvReal || MODE == kPlaneAdj ||
+                  MODE == kPlaneInvMulFwd) {
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.src + off), "r"(bytes) : "memory");
+    } else if constexpr (MODE == kPlaneAdvN) {
+      for (int c = 0; c < 3; ++c)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a.src3[c] + off), "r"(bytes) : "memory");
+    }
+  }
   const int rep = blockIdx.y;
   const int line = threadIdx.x / G, t = threadIdx.x % G;
   // row-phase scratch line: the column line buffer without a cluster or with

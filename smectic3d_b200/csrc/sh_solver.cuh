@@ -451,8 +451,13 @@ struct Solver final : SolverBase {
     return SH_OK;
   }
 
+#ifndef SHB_PLANE_PF
+#define SHB_PLANE_PF 16
+#endif
   PlaneArgs<T> plane_args() const {
     PlaneArgs<T> a{};
+    // clustered plane passes run in several waves: prefetch a later wave's planes
+    a.pf_dist = CL > 1 ? SHB_PLANE_PF : 0;
     a.tw = tw;
     a.pp = point_params();
     a.red = d_red_plane;
