@@ -1286,13 +1286,14 @@ struct Solver final : SolverBase {
       if ((rc = launch_pencil<kPencilXMul>(b))) return rc;
       const cplx<T>* src[3] = {S3[0], P, Px};
       const int mult[3] = {kMulNone, kMulNegQy2, kMulIqy};
+      PlaneArgs<T> st[3];
       for (int i = 0; i < 3; ++i) {
-        PlaneArgs<T> a = plane_args();
-        a.src = src[i];
-        a.mult = mult[i];
-        a.real_out = SR[i];
-        if ((rc = launch_plane<kPlaneInvReal>(a))) return rc;
+        st[i] = plane_args();
+        st[i].src = src[i];
+        st[i].mult = mult[i];
+        st[i].real_out = SR[i];
       }
+      if ((rc = launch_plane_sets<kPlaneInvReal>(st, 3))) return rc;
       SurfArgs<T> sa;
       sa.psi = R[0];
       sa.gx = R[1];
