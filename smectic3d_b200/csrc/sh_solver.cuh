@@ -559,7 +559,17 @@ struct Solver final : SolverBase {
   // plain steps are replayed from a CUDA graph when no per-step host
   // bookkeeping is needed
   bool graph_eligible() const {
-    return use_graphs && !prof_ms && !hist_spec && !p.energy_trace && p.l1_interval == 0;
+    return use_graphs && !prof_ms && !hist_spec && !p.energy_trace && (p.l1_interval == 0 || !blocked());
+  }
+  // with the L1 monitor on, a replayed chunk of kGraphChunk steps after step
+  // count s0 must hold neither a monitored step (count % l1_interval == 0) nor the
+  // step before one, which keeps psi for the difference
+  bool chunk_unmonitored(long long s0) const {
+    const int li = p.l1_interval;
+    if (li <= 0) return true;
+    for (long long c = s0 + 1; c <= s0 + kGraphChunk; ++c)
+      if (c % li == 0 || (c + 1) % li == 0) return false;
+    return true;
   }
   // Replica blocks (batched plain steps, replica_block = g > 0): the graph
   // advances replicas [0, g) by kGraphChunk steps, then [g, 2g), and so on, so
@@ -594,6 +604,9 @@ struct Solver final : SolverBase {
     if (graph_exec || !graph_eligible()) return SH_OK;
     cudaGraph_t g;
     const long long s0 = steps, l0 = launches;
+    // the graph holds plain steps only: the L1 monitor's steps run outside it
+    const int li = p.l1_interval;
+    p.l1_interval = 0;
     SHB_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     int rc = SH_OK;
     if (blocked()) {
@@ -607,6 +620,7 @@ struct Solver final : SolverBase {
       rc = step_direct(kGraphChunk);
     }
     cudaError_t e = cudaStreamEndCapture(stream, &g);
+    p.l1_interval = li;
     steps = s0;
     hist_pos -= kGraphChunk;
     graph_launches = launches - l0;
@@ -623,13 +637,29 @@ struct Solver final : SolverBase {
     if (graph_eligible() && n >= kGraphChunk) {
       int rc;
       if ((rc = build_graph())) return rc;
-      const int chunks = n / kGraphChunk;
-      for (int c = 0; c < chunks; ++c) {
-        SHB_CUDA(cudaGraphLaunch(graph_exec, stream));
-        steps += kGraphChunk;
-        launches += graph_launches;
+      if (p.l1_interval <= 0) {
+        const int chunks = n / kGraphChunk;
+        for (int c = 0; c < chunks; ++c) {
+          SHB_CUDA(cudaGraphLaunch(graph_exec, stream));
+          steps += kGraphChunk;
+          launches += graph_launches;
+        }
+        return step_direct(n - chunks * kGraphChunk);
       }
-      return step_direct(n - chunks * kGraphChunk);
+      // L1 monitor on (the reference's loop): replay the graph over the chunks
+      // that hold no monitored step, take the steps around each one directly
+      while (n > 0) {
+        if (n >= kGraphChunk && chunk_unmonitored(steps)) {
+          SHB_CUDA(cudaGraphLaunch(graph_exec, stream));
+          steps += kGraphChunk;
+          launches += graph_launches;
+          n -= kGraphChunk;
+        } else {
+          if ((rc = step_direct(1))) return rc;
+          --n;
+        }
+      }
+      return SH_OK;
     }
     return step_direct(n);
   }

@@ -102,3 +102,26 @@ def test_surface_step_is_bitwise_reproducible():
             outs.append(s.surface_step())
     for x, y in zip(outs[0], outs[1]):
         assert np.array_equal(x, y, equal_nan=True) if x.dtype.kind == "f" else np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("boundary", ["neumann", "periodic"])
+def test_l1_monitor_graph_replay_matches_direct_steps(boundary):
+    """With the L1 monitor on, step(n) replays the step graph between the
+    monitored steps; single steps take every step directly.  Both give the same
+    state and the same L1 values bit for bit."""
+    n = 128
+    p = S.Params(n=n, boundary=boundary, precision="fp32", dt=0.05, eps=-0.75, l1_interval=20)
+    psi0 = S.ic.noise(n, 6, amp=0.3)
+    with S.Solver(p) as a, S.Solver(p) as b:
+        a.set_psi(psi0)
+        b.set_psi(psi0)
+        la, lb = [], []
+        for _ in range(3):
+            a.step(47)
+            la.append(a.l1())
+            for _ in range(47):
+                b.step(1)
+            lb.append(b.l1())
+        assert np.array_equal(a.get_psi(), b.get_psi())
+        for x, y in zip(la, lb):
+            assert np.array_equal(np.asarray(x[0]), np.asarray(y[0])) and x[1] == y[1]
