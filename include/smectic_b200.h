@@ -110,8 +110,9 @@ int sh_step(sh_handle* h, int nsteps);
 int sh_step_async(sh_handle* h, int nsteps);
 
 /* Build ahead of time what sh_step_async replays for runs of 16 steps or
- * more without per-step diagnostics (energy_trace = 0, l1_interval = 0): a
- * CUDA graph of 16 steps, instantiated once per handle.  Runs nothing and
+ * more without an energy trace (energy_trace = 0): a CUDA graph of 16 steps,
+ * instantiated once per handle; with the L1 monitor on it replays the chunks
+ * between the monitored steps (replica blocks: only with l1_interval = 0).  Runs nothing and
  * changes no state; without this call the first such sh_step builds it.  No
  * counterpart in the reference, whose loop has no set-up beyond its FFTW plans. */
 int sh_prepare(sh_handle* h);

@@ -557,7 +557,7 @@ struct Solver final : SolverBase {
   }
 
   // plain steps are replayed from a CUDA graph when no per-step host
-  // bookkeeping is needed
+  // bookkeeping is needed (with the L1 monitor on: between its steps)
   bool graph_eligible() const {
     return use_graphs && !prof_ms && !hist_spec && !p.energy_trace && (p.l1_interval == 0 || !blocked());
   }
